@@ -1,0 +1,254 @@
+/*
+ * rocketgpu_b200 — C ABI of the B200-native batched arena tick.
+ *
+ * The drop-in boundary for the reference's BatchSim (reference include/rocketgpu/rocketgpu.h:988-1089). Plain C:
+ * opaque handle, plain pointers and sizes, int status (0 = ok) plus rg_last_error(), the convention of the
+ * reference's C shim (rust/shim/shim.h:57-78). No C++ or torch types cross it, so a pybind module, a Rust crate or a
+ * ctypes/cffi binding can sit directly on it.
+ *
+ * Public state structs are byte-identical to the reference's (same field order, types and padding), so callers pass
+ * the arrays they already hold: rg_car_state == rocketgpu::CarState (880 B), rg_ball_state == BallState (288 B),
+ * rg_env_state == EnvState (44 B), rg_boost_pad_state == BoostPadState (16 B), rg_car_controls == CarControls (24 B),
+ * rg_car_config == CarConfig (120 B), rg_env_command == EnvCommand (16 B).
+ *
+ * Device side: every rg_batch owns its device memory (one allocation per array at create time, none while stepping).
+ * Host pointers are borrowed for the call; device pointers (rg_batch_step_with_device_controls) must stay valid until
+ * the given stream has run the step. Errors are reported synchronously for argument checks; a CUDA error raised by
+ * an earlier asynchronous launch is reported by the next call that synchronises (rg_batch_synchronize, downloads).
+ */
+#ifndef ROCKETGPU_B200_H
+#define ROCKETGPU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define RG_API __declspec(dllexport)
+#else
+#define RG_API __attribute__((visibility("default")))
+#endif
+
+typedef struct rg_vec3 { float x, y, z; } rg_vec3;
+typedef struct rg_quat { float w, x, y, z; } rg_quat;
+
+/* reference rocketgpu.h:127-136 */
+typedef struct rg_car_controls {
+    float throttle, steer, pitch, yaw, roll;
+    uint8_t jump, boost, handbrake;
+} rg_car_controls;
+
+/* reference rocketgpu.h:138-171 */
+typedef struct rg_car_config {
+    rg_vec3 hitbox_size;
+    rg_vec3 hitbox_published;
+    rg_vec3 hitbox_offset;
+    rg_vec3 front_wheels_offset;
+    rg_vec3 back_wheels_offset;
+    float front_wheel_radius, back_wheel_radius;
+    float front_suspension_rest, back_suspension_rest;
+    float dodge_deadzone;
+    uint8_t three_wheels;
+    uint16_t body;
+    float steer_angle_curve_deg[6];
+    float powerslide_steer_angle_curve_deg[2];
+    float spawn_z;
+} rg_car_config;
+
+/* reference rocketgpu.h:173-184 */
+typedef struct rg_ball_hit_info {
+    uint8_t is_valid, extra_pending, extra_tick_is_previous, reserved2;
+    uint64_t tick_count_when_hit;
+    uint64_t tick_count_when_extra_impulse_applied;
+    uint32_t hit_car_id;
+    rg_vec3 relative_pos_on_ball, ball_pos, extra_hit_vel;
+} rg_ball_hit_info;
+
+/* reference rocketgpu.h:186-433 (field order and meaning as there) */
+typedef struct rg_car_state {
+    rg_vec3 pos; rg_quat rot; rg_vec3 vel; rg_vec3 ang_vel; rg_vec3 flip_rel_torque;
+    float jump_time, flip_time, air_time, air_time_since_jump, boost, time_since_boosted, boosting_time,
+        supersonic_time, handbrake_val, auto_flip_timer, boost_amount, demo_respawn_timer;
+    uint64_t tick_count_since_update;
+    uint8_t ball_contact_last_tick, ball_contact_this_tick;
+    uint8_t is_on_ground;
+    uint8_t wheels_with_contact[4];
+    uint8_t has_jumped, has_double_jumped, has_flipped, is_flipping, is_jumping, is_boosting, is_supersonic,
+        is_auto_flipping, is_demoed, just_respawned;
+    uint8_t demo_no_contact_response, respawn_slot_override_plus1, rlbotv5_boost_hold;
+    struct { uint8_t has_contact, wheel_ball_mask, reserved1, reserved2; rg_vec3 contact_normal; } world_contact;
+    struct { uint32_t other_car_id; float cooldown_timer; } car_contact;
+    rg_vec3 vel_impulse_cache;
+    rg_ball_hit_info ball_hit_info;
+    rg_car_controls last_controls;
+    rg_vec3 pos_bt, vel_bt, tick_start_pos_bt, pad_frame_pos_bt;
+    uint8_t vel_touched_solve_stage, basis_authoritative, ext_force_impulse_bt_valid, pad_frame_pos_valid;
+    rg_vec3 basis_forward, basis_right, basis_up;
+    rg_vec3 ext_force_impulse_bt, ext_torque_impulse, solve_delta_linear_bt, vel_impulse_cache_bt, solve_delta_angular;
+    uint8_t bump_event_bumps[7], bump_event_demos[7];
+    uint8_t boost_pad_touching, bump_event_reserved1;
+    uint64_t previous_ball_contact_start, last_ball_contact_start, last_world_surface_contact,
+        first_world_after_previous_ball, first_world_after_last_ball, last_flip_or_jump_start,
+        last_directional_flip_start;
+    uint8_t last_ball_started_with_world, flip_or_jump_last_tick;
+    float internal_jump_time, internal_flip_time;
+    uint8_t flip_timer_live;
+    uint8_t air_state;
+    uint16_t driving_disabled;
+    float dodge_timeout, dodge_elapsed, dodge_dir_x, dodge_dir_y;
+    uint64_t latest_touch_tick;
+    rg_vec3 latest_touch_location, latest_touch_normal;
+    rg_vec3 internal_vel, internal_ang_vel, reported_vel, reported_ang_vel;
+    uint8_t internal_has_jumped, internal_has_double_jumped, internal_has_flipped, internal_is_supersonic,
+        reported_flags, game_has_jumped, double_jump_ticks, jump_hold_broken, supersonic_set_v3, rlbotv5_dodged;
+    rg_vec3 set_wheel_normals[4];
+    uint8_t set_wheel_normals_mask, cal_pre_flags;
+    float cal_pre_forward_speed_uu, cal_pre_pitchlock_restart_time;
+    rg_vec3 cal_tick_start_ang_vel, tick_start_basis_forward, tick_start_basis_right, tick_start_basis_up;
+    rg_vec3 restored_inv_inertia_bt[3];
+    uint8_t restored_inv_inertia_valid;
+    rg_vec3 pending_bump_bt[7];
+    uint32_t pending_bump_hitter[7];
+    uint8_t pending_bump_count;
+    float auto_flip_torque_scale;
+} rg_car_state;
+
+/* reference rocketgpu.h:435-505 */
+typedef struct rg_ball_state {
+    struct { float y_target_dir, cur_target_speed, time_since_hit; } hs_info;
+    struct {
+        int32_t charge_level; float accumulated_hit_force, y_target_dir;
+        uint8_t has_damaged, reserved0, reserved1, reserved2;
+        uint64_t last_damage_tick;
+    } ds_info;
+    rg_vec3 pos; rg_quat rot; rg_vec3 vel; rg_vec3 ang_vel; rg_vec3 vel_impulse_cache;
+    uint64_t tick_count_when_extra_impulse_applied;
+    uint64_t tick_count_since_update;
+    rg_vec3 pos_bt, vel_bt;
+    rg_vec3 basis_forward, basis_right, basis_up;
+    uint32_t basis_authoritative;
+    rg_vec3 inertia_basis_forward, inertia_basis_right, inertia_basis_up;
+    uint32_t inertia_basis_valid;
+    rg_vec3 restored_inv_inertia_bt[3];
+    uint32_t restored_inv_inertia_valid;
+    rg_vec3 vel_impulse_cache_bt;
+    uint32_t sleeping;
+    float deactivation_time;
+    uint16_t constrained_2d, reserved_c2d;
+} rg_ball_state;
+
+/* reference rocketgpu.h:507-516 */
+typedef struct rg_boost_pad_state {
+    float cooldown;
+    uint8_t is_active, is_big;
+    uint16_t pickup_frac_q;
+    uint32_t prev_locked_car_id, cur_locked_car_id;
+} rg_boost_pad_state;
+
+/* reference rocketgpu.h:535-575 */
+typedef struct rg_env_state {
+    uint32_t tick, blue_score, orange_score;
+    int32_t last_scored_team;
+    uint8_t goal_scored_this_tick, car_visit_order_mode, car_visit_present_mask, kickoff_resets;
+    uint32_t car_visit_order_packed;
+    uint8_t countdown_phase, countdown_fires;
+    uint16_t frame_ticks;
+    float countdown_count, frame_frac_prev;
+    uint16_t kickoff_match_order;
+    uint8_t kickoff_match_index, goal_latched, respawn_match_order;
+} rg_env_state;
+
+/* reference rocketgpu.h:683-706 */
+typedef struct rg_env_command {
+    uint8_t reset_to_kickoff, reset_scoreboard, reset_tick_count, kickoff_seed_mode, new_round_bodies, keep_boost_pads;
+    uint16_t kickoff_countdown_ticks;
+    uint64_t kickoff_seed;
+} rg_env_command;
+
+/* The BatchSim configuration subset this path takes (reference SimConfig, rocketgpu.h:842-909, and the
+ * MutatorConfig fields the tick reads, rocketgpu.h:708-840). Zero-initialise, then call rg_sim_config_default. */
+typedef struct rg_sim_config {
+    int32_t env_count;
+    int32_t max_cars_per_env;       /* 0..8 */
+    float tick_dt;                   /* 1/120 */
+    uint8_t enable_boost_pads, enable_car_car_collisions, enable_demos, enable_scoring;
+    uint64_t respawn_rng_seed;
+    /* mutator */
+    float gravity_z, ball_radius, ball_mass, car_mass, ball_drag, ball_friction, ball_restitution, ball_max_speed,
+        ball_max_ang_speed, car_max_speed, car_max_ang_speed, arena_friction, arena_restitution,
+        goal_base_threshold_y;
+    uint8_t kickoff_settled;
+    uint8_t reserved[7];
+} rg_sim_config;
+
+/* A custom arena (reference ArenaLayout, rocketgpu.h:943-959): one triangle mesh in uu; pads, goals and spawns are
+ * the official soccar ones. */
+typedef struct rg_arena_layout {
+    const float* vertices_uu;   /* 3 * vertex_count */
+    int64_t vertex_count;
+    const int32_t* indices;     /* 3 per triangle */
+    int64_t index_count;
+} rg_arena_layout;
+
+typedef struct rg_batch rg_batch;
+
+/* Last error of this thread, "" if none. */
+RG_API const char* rg_last_error(void);
+/* Library version string. */
+RG_API const char* rg_version(void);
+
+/* Fills a config with the reference's SimConfig/MutatorConfig defaults. */
+RG_API void rg_sim_config_default(rg_sim_config* cfg);
+/* Reference-default public states (the reference's member initialisers), for callers building uploads. */
+RG_API void rg_default_ball_state(rg_ball_state* out);
+RG_API void rg_default_env_state(rg_env_state* out);
+
+/* BatchSim(config, layout) — reference rocketgpu.h:990-992, src/rocketgpu.cpp:1019-1250. Validates the config
+ * (env_count > 0, 0 <= max_cars_per_env <= 8) and layout (finite, within 11,500 uu), builds the mesh BVH on the
+ * host, uploads it and allocates every device array. */
+RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layout, int device, rg_batch** out);
+/* ~BatchSim */
+RG_API void rg_batch_destroy(rg_batch* b);
+
+RG_API int64_t rg_batch_env_count(const rg_batch* b);    /* BatchSim::env_count (rocketgpu.h:1012) */
+RG_API int64_t rg_batch_car_capacity(const rg_batch* b); /* BatchSim::car_capacity (rocketgpu.h:1011) */
+
+/* BatchSim::set_env_car_count (rocketgpu.h:1017; range checks src/rocketgpu.cpp:2920-2932). */
+RG_API int rg_batch_set_env_car_count(rg_batch* b, const int32_t* host_counts, size_t count, void* stream);
+/* BatchSim::upload_ball_states / download_ball_states (rocketgpu.h:1023-1046). */
+RG_API int rg_batch_upload_ball_states(rg_batch* b, const rg_ball_state* host, size_t count, void* stream);
+RG_API int rg_batch_download_ball_states(rg_batch* b, rg_ball_state* host, size_t count, void* stream);
+/* BatchSim::upload_env_states / download_env_states (rocketgpu.h:1027,1047). */
+RG_API int rg_batch_upload_env_states(rg_batch* b, const rg_env_state* host, size_t count, void* stream);
+RG_API int rg_batch_download_env_states(rg_batch* b, rg_env_state* host, size_t count, void* stream);
+
+/* BatchSim::step (rocketgpu.h:1063; src/rocketgpu.cpp:3237): advances every env by `ticks` 120 Hz ticks on `stream`
+ * (asynchronous; no host synchronisation). */
+RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream);
+
+/* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
+RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
+
+/* The reference's single-precision transcendental routines as the tick evaluates them (reference
+ * include/rocketgpu/detail/math.hpp:39-457: UCRT-compatible sinf, cosf, atan2f, powf), for host code that must
+ * reproduce the tick's arithmetic (e.g. a config's cached drag factor). */
+RG_API float rg_ucrt_sinf(float x);
+RG_API float rg_ucrt_cosf(float x);
+RG_API float rg_ucrt_atan2f(float y, float x);
+RG_API float rg_ucrt_powf(float x, float y);
+
+/* Device arrays (reference DeviceView, rocketgpu.h:961-986); non-owning, valid until rg_batch_destroy. */
+typedef struct rg_device_view {
+    void* ball_states;       /* rg_ball_state[env_count] */
+    void* env_states;        /* rg_env_state[env_count] */
+    int32_t* env_car_count;  /* [env_count] */
+} rg_device_view;
+RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ROCKETGPU_B200_H */

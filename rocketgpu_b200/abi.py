@@ -1,0 +1,85 @@
+"""ctypes binding of include/rocketgpu_b200.h (the in-tree CUDA library rocketgpu_b200/_lib/librocketgpu_b200.so).
+
+This is the binding a ctypes/cffi user of the C ABI writes; the pybind / Rust shims of the reference would bind the
+same symbols.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "librocketgpu_b200.so")
+
+# Every symbol include/rocketgpu_b200.h declares.
+EXPORTS = [
+    "rg_last_error", "rg_version", "rg_sim_config_default", "rg_default_ball_state", "rg_default_env_state",
+    "rg_batch_create", "rg_batch_destroy", "rg_batch_env_count", "rg_batch_car_capacity",
+    "rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
+    "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_step", "rg_batch_synchronize",
+    "rg_batch_device_view", "rg_ucrt_sinf", "rg_ucrt_cosf", "rg_ucrt_atan2f", "rg_ucrt_powf",
+]
+
+
+class rg_sim_config(ctypes.Structure):
+    _fields_ = [
+        ("env_count", ctypes.c_int32), ("max_cars_per_env", ctypes.c_int32), ("tick_dt", ctypes.c_float),
+        ("enable_boost_pads", ctypes.c_uint8), ("enable_car_car_collisions", ctypes.c_uint8),
+        ("enable_demos", ctypes.c_uint8), ("enable_scoring", ctypes.c_uint8),
+        ("respawn_rng_seed", ctypes.c_uint64),
+        ("gravity_z", ctypes.c_float), ("ball_radius", ctypes.c_float), ("ball_mass", ctypes.c_float),
+        ("car_mass", ctypes.c_float), ("ball_drag", ctypes.c_float), ("ball_friction", ctypes.c_float),
+        ("ball_restitution", ctypes.c_float), ("ball_max_speed", ctypes.c_float),
+        ("ball_max_ang_speed", ctypes.c_float), ("car_max_speed", ctypes.c_float),
+        ("car_max_ang_speed", ctypes.c_float), ("arena_friction", ctypes.c_float),
+        ("arena_restitution", ctypes.c_float), ("goal_base_threshold_y", ctypes.c_float),
+        ("kickoff_settled", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 7),
+    ]
+
+
+class rg_arena_layout(ctypes.Structure):
+    _fields_ = [("vertices_uu", ctypes.POINTER(ctypes.c_float)), ("vertex_count", ctypes.c_int64),
+                ("indices", ctypes.POINTER(ctypes.c_int32)), ("index_count", ctypes.c_int64)]
+
+
+class rg_device_view(ctypes.Structure):
+    _fields_ = [("ball_states", ctypes.c_void_p), ("env_states", ctypes.c_void_p),
+                ("env_car_count", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library (raises if it is not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"rocketgpu_b200 CUDA library not built ({LIB_PATH}); run python -m rocketgpu_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i64, sz, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_size_t, ctypes.c_int32
+        L.rg_last_error.restype = ctypes.c_char_p
+        L.rg_version.restype = ctypes.c_char_p
+        L.rg_sim_config_default.argtypes = [vp]
+        L.rg_default_ball_state.argtypes = [vp]
+        L.rg_default_env_state.argtypes = [vp]
+        L.rg_batch_create.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.rg_batch_destroy.argtypes = [vp]
+        L.rg_batch_env_count.argtypes = [vp]
+        L.rg_batch_env_count.restype = i64
+        L.rg_batch_car_capacity.argtypes = [vp]
+        L.rg_batch_car_capacity.restype = i64
+        for n in ("rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
+                  "rg_batch_upload_env_states", "rg_batch_download_env_states"):
+            getattr(L, n).argtypes = [vp, vp, sz, vp]
+        L.rg_batch_step.argtypes = [vp, i32, vp]
+        L.rg_batch_synchronize.argtypes = [vp, vp]
+        L.rg_batch_device_view.argtypes = [vp, vp]
+        for n in ("rg_ucrt_sinf", "rg_ucrt_cosf"):
+            getattr(L, n).argtypes = [ctypes.c_float]
+            getattr(L, n).restype = ctypes.c_float
+        for n in ("rg_ucrt_atan2f", "rg_ucrt_powf"):
+            getattr(L, n).argtypes = [ctypes.c_float, ctypes.c_float]
+            getattr(L, n).restype = ctypes.c_float
+        _lib = L
+    return _lib

@@ -1,0 +1,120 @@
+"""Python mirror of the reference's BatchSim (include/rocketgpu/rocketgpu.h:988-1089) over the C ABI.
+
+The methods keep the reference's names and argument meaning (state arrays are the byte-identical public structs, as
+numpy uint8 rows or structured arrays); errors raise the reference's exception types: ValueError for
+std::invalid_argument, IndexError for std::out_of_range, RuntimeError for CUDA errors.
+
+There is no CPU fallback: loading fails loudly when the CUDA library is missing or no GPU is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import abi
+
+CAR_BYTES, BALL_BYTES, ENV_BYTES = 880, 288, 44
+
+
+def _check(rc: int):
+    if rc == 0:
+        return
+    msg = abi.lib().rg_last_error().decode()
+    if rc == 2:
+        raise ValueError(msg)
+    if rc == 3:
+        raise IndexError(msg)
+    raise RuntimeError(msg)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class SimConfig:
+    """The reference SimConfig / MutatorConfig fields this path takes (defaults as the reference's)."""
+
+    def __init__(self, env_count: int = 1, max_cars_per_env: int = 6, **kw):
+        c = abi.rg_sim_config()
+        abi.lib().rg_sim_config_default(ctypes.byref(c))
+        c.env_count = env_count
+        c.max_cars_per_env = max_cars_per_env
+        for k, v in kw.items():
+            if not hasattr(c, k):
+                raise ValueError(f"unknown SimConfig field {k}")
+            setattr(c, k, v)
+        self.c = c
+
+
+class BatchSim:
+    """N independent arenas on one GPU, stepped by whole 120 Hz ticks.
+
+    `vertices` (float32 [V, 3], uu) and `indices` (int32 [3T]) are the arena's triangle mesh (ArenaLayout.meshes[0]).
+    """
+
+    def __init__(self, config: SimConfig, vertices: np.ndarray, indices: np.ndarray, device: int = 0):
+        self._v = np.ascontiguousarray(vertices, np.float32)
+        self._i = np.ascontiguousarray(indices, np.int32)
+        lay = abi.rg_arena_layout()
+        lay.vertices_uu = self._v.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        lay.vertex_count = len(self._v)
+        lay.indices = self._i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        lay.index_count = len(self._i)
+        h = ctypes.c_void_p()
+        _check(abi.lib().rg_batch_create(ctypes.byref(config.c), ctypes.byref(lay), device, ctypes.byref(h)))
+        self._h = h
+        self.config = config
+
+    def close(self):
+        if getattr(self, "_h", None):
+            abi.lib().rg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def env_count(self) -> int:
+        return abi.lib().rg_batch_env_count(self._h)
+
+    def car_capacity(self) -> int:
+        return abi.lib().rg_batch_car_capacity(self._h)
+
+    def set_env_car_count(self, counts, stream: int = 0):
+        c = np.ascontiguousarray(counts, np.int32)
+        _check(abi.lib().rg_batch_set_env_car_count(self._h, _ptr(c), len(c), stream))
+
+    def upload_ball_states(self, states: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(states, np.uint8).reshape(-1, BALL_BYTES)
+        _check(abi.lib().rg_batch_upload_ball_states(self._h, _ptr(s), len(s), stream))
+
+    def download_ball_states(self, count: int | None = None, stream: int = 0) -> np.ndarray:
+        n = self.env_count() if count is None else count
+        out = np.zeros((n, BALL_BYTES), np.uint8)
+        _check(abi.lib().rg_batch_download_ball_states(self._h, _ptr(out), n, stream))
+        return out
+
+    def upload_env_states(self, states: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(states, np.uint8).reshape(-1, ENV_BYTES)
+        _check(abi.lib().rg_batch_upload_env_states(self._h, _ptr(s), len(s), stream))
+
+    def download_env_states(self, count: int | None = None, stream: int = 0) -> np.ndarray:
+        n = self.env_count() if count is None else count
+        out = np.zeros((n, ENV_BYTES), np.uint8)
+        _check(abi.lib().rg_batch_download_env_states(self._h, _ptr(out), n, stream))
+        return out
+
+    def step(self, ticks: int = 1, stream: int = 0):
+        _check(abi.lib().rg_batch_step(self._h, ticks, stream))
+
+    def synchronize(self, stream: int = 0):
+        _check(abi.lib().rg_batch_synchronize(self._h, stream))
+
+    def device_view(self) -> dict:
+        v = abi.rg_device_view()
+        _check(abi.lib().rg_batch_device_view(self._h, ctypes.byref(v)))
+        return {"ball_states": v.ball_states, "env_states": v.env_states, "env_car_count": v.env_car_count}

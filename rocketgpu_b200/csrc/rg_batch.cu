@@ -1,0 +1,398 @@
+// rg_batch: the C ABI (include/rocketgpu_b200.h) and the sm_100a kernels behind it.
+//
+// Execution model. One CUDA thread owns one arena for the whole launch: it loads the arena's ball and env state from
+// HBM once, runs `ticks` ticks with the state in registers, and stores it back once. Arenas are independent (the
+// reference steps each env in isolation, include/rocketgpu/detail/step/env_step.hpp:7048), so a step is one launch
+// over ceil(envs / 128) blocks with no inter-thread communication; at 16K arenas that is ~128 blocks, under one wave
+// of the 148 SMs. Ticks per launch amortise the state load/store and launch latency.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rg_mesh.h"
+#include "rg_tick.cuh"
+#include "rg_ucrt.cuh"
+#include "rocketgpu_b200.h"
+
+namespace {
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = std::string("invalid_argument: ") + e.what();
+        return 2;
+    } catch (const std::out_of_range& e) {
+        g_last_error = std::string("out_of_range: ") + e.what();
+        return 3;
+    } catch (const CudaError& e) {
+        g_last_error = std::string("cuda: ") + e.what();
+        return 4;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 1;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return 1;
+    }
+}
+
+template <class T>
+struct DeviceArray {
+    T* ptr = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        if (count) check(cudaMalloc(&ptr, count * sizeof(T)), "cudaMalloc");
+    }
+    ~DeviceArray() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+}  // namespace
+
+struct rg_batch {
+    int device = 0;
+    rg_sim_config cfg{};
+    rg::TickConfig tc{};
+    int32_t env_count = 0;
+    int32_t max_cars = 0;
+    DeviceArray<rg::BallState> balls;
+    DeviceArray<rg::EnvState> envs;
+    DeviceArray<int32_t> env_car_count;
+    rg::MeshHost mesh_host;
+    rg::MeshDevice mesh;
+    std::vector<int32_t> host_car_count;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) check(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Ball import: uu -> bt with the reference's one-ulp nudge so bt * 50 reproduces the uploaded uu value exactly, then
+// uu recomputed from bt; the ball is marked "just uploaded" (sleeping = 2) (reference CanonicalizeImportedBallStates,
+// src/rocketgpu.cpp:325-382).
+__device__ float imported_linear_bt(float value) {
+    const float bt = value * (1.0f / 50.0f);
+    if (bt * 50.0f == value) return bt;
+    const float up = nextafterf(bt, INFINITY);
+    const float down = nextafterf(bt, -INFINITY);
+    if (up * 50.0f == value) return up;
+    if (down * 50.0f == value) return down;
+    return bt;
+}
+
+__global__ void canonicalize_balls_kernel(rg::BallState* balls, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rg::BallState& b = balls[i];
+    b.pos_bt = rg::V3{imported_linear_bt(b.pos.x), imported_linear_bt(b.pos.y), imported_linear_bt(b.pos.z)};
+    b.vel_bt = rg::V3{imported_linear_bt(b.vel.x), imported_linear_bt(b.vel.y), imported_linear_bt(b.vel.z)};
+    b.pos = b.pos_bt * 50.0f;
+    b.vel = b.vel_bt * 50.0f;
+    b.sleeping = 2;
+    b.deactivation_time = 0.0f;
+}
+
+struct TickArgs {
+    rg::BallState* balls;
+    rg::EnvState* envs;
+    const int32_t* env_car_count;
+    int32_t env_count;
+    rg::TickConfig tc;
+    rg::MeshDevice mesh;
+};
+
+__global__ void __launch_bounds__(128) tick_kernel(TickArgs a, int ticks) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.env_count) return;
+    rg::BallState b = a.balls[e];
+    rg::EnvState env = a.envs[e];
+    for (int t = 0; t < ticks; ++t) {
+        rg::arena_tick(env, b, a.tc, a.mesh);
+    }
+    a.balls[e] = b;
+    a.envs[e] = env;
+}
+
+void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
+    TickArgs a;
+    a.balls = b->balls.ptr;
+    a.envs = b->envs.ptr;
+    a.env_car_count = b->env_car_count.ptr;
+    a.env_count = b->env_count;
+    a.tc = b->tc;
+    a.mesh = b->mesh;
+    const int threads = 128;
+    const int blocks = (b->env_count + threads - 1) / threads;
+    tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
+    check(cudaGetLastError(), "tick_kernel launch");
+}
+
+rg::TickConfig resolve_tick_config(const rg_sim_config& c) {
+    rg::TickConfig t{};
+    t.tick_dt = c.tick_dt;
+    t.gravity_z = c.gravity_z;
+    t.ball_radius = c.ball_radius;
+    t.ball_mass = c.ball_mass;
+    t.ball_drag = c.ball_drag;
+    // BatchSim caches the per-tick drag factor (1 - drag)^dt once per config (reference CacheBallDamping,
+    // src/rocketgpu.cpp:259-270).
+    t.ball_drag_scale = c.ball_drag <= 0.0f ? 1.0f : rg::ucrt_powf(rg::fmax_(0.0f, 1.0f - c.ball_drag), c.tick_dt);
+    t.ball_friction = c.ball_friction;
+    t.ball_restitution = c.ball_restitution;
+    t.ball_max_speed = c.ball_max_speed;
+    t.ball_max_ang_speed = c.ball_max_ang_speed;
+    t.goal_base_threshold_y = c.goal_base_threshold_y;
+    t.frame_frac = 0.5f;
+    t.enable_scoring = c.enable_scoring;
+    return t;
+}
+
+}  // namespace
+
+extern "C" {
+
+RG_API const char* rg_last_error(void) { return g_last_error.c_str(); }
+RG_API const char* rg_version(void) { return "rocketgpu_b200 0.1 (sm_100a)"; }
+
+RG_API void rg_sim_config_default(rg_sim_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->env_count = 1;
+    c->max_cars_per_env = 6;
+    c->tick_dt = 1.0f / 120.0f;
+    c->enable_boost_pads = 1;
+    c->enable_car_car_collisions = 1;
+    c->enable_demos = 1;
+    c->enable_scoring = 1;
+    c->gravity_z = -650.0f;
+    c->ball_radius = 91.24999f;
+    c->ball_mass = 30.000002f;
+    c->car_mass = 180.0f;
+    c->ball_drag = 0.03f;
+    c->ball_friction = 0.35f;
+    c->ball_restitution = 0.60f;
+    c->ball_max_speed = 6000.0f;
+    c->ball_max_ang_speed = 6.0f;
+    c->car_max_speed = 2300.0f;
+    c->car_max_ang_speed = 5.5f;
+    c->arena_friction = 0.30f;
+    c->arena_restitution = 0.30f;
+    c->goal_base_threshold_y = 5124.2373046875f;
+    c->kickoff_settled = 1;
+}
+
+RG_API void rg_default_ball_state(rg_ball_state* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->hs_info.cur_target_speed = 2900.0f;
+    o->ds_info.charge_level = 1;
+    o->pos = {0.0f, 0.0f, 93.15f};
+    o->rot = {1.0f, 0.0f, 0.0f, 0.0f};
+    o->pos_bt = {0.0f, 0.0f, 93.15f * (1.0f / 50.0f)};
+    o->basis_forward = {1.0f, 0.0f, 0.0f};
+    o->basis_right = {0.0f, 1.0f, 0.0f};
+    o->basis_up = {0.0f, 0.0f, 1.0f};
+    o->inertia_basis_forward = {1.0f, 0.0f, 0.0f};
+    o->inertia_basis_right = {0.0f, 1.0f, 0.0f};
+    o->inertia_basis_up = {0.0f, 0.0f, 1.0f};
+}
+
+RG_API void rg_default_env_state(rg_env_state* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->last_scored_team = -1;
+    o->car_visit_order_mode = 3;
+    o->car_visit_present_mask = 0xFF;
+    o->car_visit_order_packed = 0x76543210u;
+    o->frame_frac_prev = 0.5f;
+}
+
+RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layout, int device, rg_batch** out) {
+    return guard([&] {
+        if (!cfg || !layout || !out) throw std::invalid_argument("null argument");
+        if (cfg->env_count <= 0) throw std::invalid_argument("env_count must be positive");
+        if (cfg->max_cars_per_env < 0 || cfg->max_cars_per_env > 8)
+            throw std::invalid_argument("max_cars_per_env must be in [0, 8]");
+        if (!(cfg->tick_dt > 0.0f)) throw std::invalid_argument("tick_dt must be positive");
+        std::unique_ptr<rg_batch> b(new rg_batch);
+        b->device = device;
+        b->cfg = *cfg;
+        b->env_count = cfg->env_count;
+        b->max_cars = cfg->max_cars_per_env;
+        b->tc = resolve_tick_config(*cfg);
+        b->mesh_host = rg::build_mesh_host(layout->vertices_uu, layout->vertex_count, layout->indices,
+                                           layout->index_count);
+        DeviceGuard dg(device);
+        b->mesh = rg::upload_mesh(b->mesh_host);
+        b->balls.alloc(b->env_count);
+        b->envs.alloc(b->env_count);
+        b->env_car_count.alloc(b->env_count);
+        std::vector<rg_ball_state> balls(b->env_count);
+        std::vector<rg_env_state> envs(b->env_count);
+        for (auto& x : balls) rg_default_ball_state(&x);
+        for (auto& x : envs) rg_default_env_state(&x);
+        b->host_car_count.assign(b->env_count, 0);
+        check(cudaMemcpy(b->balls.ptr, balls.data(), balls.size() * sizeof(rg_ball_state), cudaMemcpyHostToDevice),
+              "upload balls");
+        check(cudaMemcpy(b->envs.ptr, envs.data(), envs.size() * sizeof(rg_env_state), cudaMemcpyHostToDevice),
+              "upload envs");
+        check(cudaMemcpy(b->env_car_count.ptr, b->host_car_count.data(), b->env_count * sizeof(int32_t),
+                         cudaMemcpyHostToDevice),
+              "upload car counts");
+        *out = b.release();
+    });
+}
+
+RG_API void rg_batch_destroy(rg_batch* b) {
+    if (!b) return;
+    DeviceGuard dg(b->device);
+    rg::free_mesh(b->mesh);
+    delete b;
+}
+
+RG_API int64_t rg_batch_env_count(const rg_batch* b) { return b ? b->env_count : 0; }
+RG_API int64_t rg_batch_car_capacity(const rg_batch* b) {
+    return b ? static_cast<int64_t>(b->env_count) * b->max_cars : 0;
+}
+
+RG_API int rg_batch_set_env_car_count(rg_batch* b, const int32_t* counts, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!counts && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("set_env_car_count count exceeds env_count");
+        for (size_t i = 0; i < count; ++i) {
+            if (counts[i] < 0 || counts[i] > b->max_cars)
+                throw std::out_of_range("env car count out of range [0, max_cars_per_env]");
+            if (counts[i] != 0)
+                throw std::invalid_argument("this build steps ball-only arenas: env car counts must be 0");
+        }
+        DeviceGuard dg(b->device);
+        std::memcpy(b->host_car_count.data(), counts, count * sizeof(int32_t));
+        check(cudaMemcpyAsync(b->env_car_count.ptr, counts, count * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              static_cast<cudaStream_t>(stream)),
+              "set_env_car_count");
+        check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "set_env_car_count sync");
+    });
+}
+
+RG_API int rg_batch_upload_ball_states(rg_batch* b, const rg_ball_state* host, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!host && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("upload_ball_states count exceeds env_count");
+        if (!count) return;
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(b->balls.ptr, host, count * sizeof(rg_ball_state), cudaMemcpyHostToDevice, s),
+              "upload_ball_states");
+        canonicalize_balls_kernel<<<(static_cast<int>(count) + 127) / 128, 128, 0, s>>>(b->balls.ptr,
+                                                                                        static_cast<int>(count));
+        check(cudaGetLastError(), "canonicalize launch");
+        check(cudaStreamSynchronize(s), "upload_ball_states sync");
+    });
+}
+
+RG_API int rg_batch_download_ball_states(rg_batch* b, rg_ball_state* host, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!host && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("download_ball_states count exceeds env_count");
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(host, b->balls.ptr, count * sizeof(rg_ball_state), cudaMemcpyDeviceToHost, s),
+              "download_ball_states");
+        check(cudaStreamSynchronize(s), "download_ball_states sync");
+    });
+}
+
+RG_API int rg_batch_upload_env_states(rg_batch* b, const rg_env_state* host, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!host && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("upload_env_states count exceeds env_count");
+        for (size_t i = 0; i < count; ++i) {
+            const uint8_t m = host[i].car_visit_order_mode;
+            if (m > 3) throw std::invalid_argument("upload_env_states: car_visit_order_mode must be 0, 1, 2 or 3");
+        }
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(b->envs.ptr, host, count * sizeof(rg_env_state), cudaMemcpyHostToDevice, s),
+              "upload_env_states");
+        check(cudaStreamSynchronize(s), "upload_env_states sync");
+    });
+}
+
+RG_API int rg_batch_download_env_states(rg_batch* b, rg_env_state* host, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!host && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("download_env_states count exceeds env_count");
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(host, b->envs.ptr, count * sizeof(rg_env_state), cudaMemcpyDeviceToHost, s),
+              "download_env_states");
+        check(cudaStreamSynchronize(s), "download_env_states sync");
+    });
+}
+
+RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        if (ticks < 0) throw std::invalid_argument("ticks must be >= 0");
+        if (ticks == 0) return;
+        DeviceGuard dg(b->device);
+        launch_tick(b, ticks, static_cast<cudaStream_t>(stream));
+    });
+}
+
+RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        DeviceGuard dg(b->device);
+        check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
+    });
+}
+
+RG_API float rg_ucrt_sinf(float x) { return rg::game_sinf(x); }
+RG_API float rg_ucrt_cosf(float x) { return rg::game_cosf(x); }
+RG_API float rg_ucrt_atan2f(float y, float x) { return rg::ucrt_atan2f(y, x); }
+RG_API float rg_ucrt_powf(float x, float y) { return rg::ucrt_powf(x, y); }
+
+RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out) {
+    return guard([&] {
+        if (!b || !out) throw std::invalid_argument("null argument");
+        out->ball_states = b->balls.ptr;
+        out->env_states = b->envs.ptr;
+        out->env_car_count = b->env_car_count.ptr;
+    });
+}
+
+}  // extern "C"

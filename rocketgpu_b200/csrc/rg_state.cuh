@@ -1,0 +1,71 @@
+// Device views of the public state structs (byte-identical to the C ABI's rg_*_state, which are byte-identical to the
+// reference's BallState / EnvState, include/rocketgpu/rocketgpu.h:435-575) plus the per-config constants the tick
+// reads.
+#pragma once
+
+#include <stddef.h>
+
+#include "rg_math.cuh"
+#include "rocketgpu_b200.h"
+
+namespace rg {
+
+struct BallState {
+    float hs_y_target_dir, hs_cur_target_speed, hs_time_since_hit;
+    uint32_t ds_pad0;
+    int32_t ds_charge_level;
+    float ds_accumulated_hit_force, ds_y_target_dir;
+    uint8_t ds_flags[4];
+    uint64_t ds_last_damage_tick;
+    V3 pos;
+    Q4 rot;
+    V3 vel;
+    V3 ang_vel;
+    V3 vel_impulse_cache;
+    uint64_t tick_count_when_extra_impulse_applied;
+    uint64_t tick_count_since_update;
+    V3 pos_bt, vel_bt;
+    V3 basis_forward, basis_right, basis_up;
+    uint32_t basis_authoritative;
+    V3 inertia_basis_forward, inertia_basis_right, inertia_basis_up;
+    uint32_t inertia_basis_valid;
+    V3 restored_inv_inertia_bt[3];
+    uint32_t restored_inv_inertia_valid;
+    V3 vel_impulse_cache_bt;
+    uint32_t sleeping;
+    float deactivation_time;
+    uint16_t constrained_2d, reserved_c2d;
+};
+static_assert(sizeof(BallState) == sizeof(rg_ball_state), "BallState layout");
+static_assert(offsetof(BallState, pos) == offsetof(rg_ball_state, pos), "BallState layout");
+static_assert(offsetof(BallState, vel_bt) == offsetof(rg_ball_state, vel_bt), "BallState layout");
+static_assert(offsetof(BallState, sleeping) == offsetof(rg_ball_state, sleeping), "BallState layout");
+static_assert(offsetof(BallState, constrained_2d) == offsetof(rg_ball_state, constrained_2d), "BallState layout");
+
+struct EnvState {
+    uint32_t tick, blue_score, orange_score;
+    int32_t last_scored_team;
+    uint8_t goal_scored_this_tick, car_visit_order_mode, car_visit_present_mask, kickoff_resets;
+    uint32_t car_visit_order_packed;
+    uint8_t countdown_phase, countdown_fires;
+    uint16_t frame_ticks;
+    float countdown_count, frame_frac_prev;
+    uint16_t kickoff_match_order;
+    uint8_t kickoff_match_index, goal_latched, respawn_match_order;
+};
+static_assert(sizeof(EnvState) == sizeof(rg_env_state), "EnvState layout");
+static_assert(offsetof(EnvState, frame_frac_prev) == offsetof(rg_env_state, frame_frac_prev), "EnvState layout");
+
+// Constants of one BatchSim config, resolved on the host (the reference's SimConfig + MutatorConfig fields the tick
+// reads, with BatchSim's derived values such as the cached per-tick drag factor).
+struct TickConfig {
+    float tick_dt;
+    float gravity_z;
+    float ball_radius, ball_mass, ball_drag, ball_drag_scale, ball_friction, ball_restitution;
+    float ball_max_speed, ball_max_ang_speed;
+    float goal_base_threshold_y;
+    float frame_frac;
+    uint8_t enable_scoring;
+};
+
+}  // namespace rg

@@ -1,0 +1,68 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every declared symbol, its structs are byte-identical
+to the reference's, and argument validation fails the way the reference's BatchSim does. No GPU calls."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from rocketgpu_b200 import abi
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.lib()
+    header = open(abi.os.path.join(abi.HERE, "..", "include", "rocketgpu_b200.h")).read()
+    declared = set(re.findall(r"RG_API\s+[\w\s\*]+?\b(rg_\w+)\s*\(", header))
+    assert declared == set(abi.EXPORTS), declared ^ set(abi.EXPORTS)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_defaults_match_reference_structs(oracle_available):
+    from tests import oracle_ref
+    lib = abi.lib()
+    car, ball, env, pad, cfg = oracle_ref.default_states()
+    my_ball = np.zeros(288, np.uint8)
+    my_env = np.zeros(44, np.uint8)
+    lib.rg_default_ball_state(my_ball.ctypes.data)
+    lib.rg_default_env_state(my_env.ctypes.data)
+    assert bytes(my_ball) == bytes(ball)
+    assert bytes(my_env) == bytes(env)
+
+
+def test_ucrt_math_matches_reference(oracle_available):
+    from tests import oracle_ref
+    L = oracle_ref.lib()
+    for f in (L.orc_ucrt_powf, L.orc_ucrt_atan2f):
+        f.restype = ctypes.c_float
+        f.argtypes = [ctypes.c_float, ctypes.c_float]
+    for f in (L.orc_ucrt_sinf, L.orc_ucrt_cosf):
+        f.restype = ctypes.c_float
+        f.argtypes = [ctypes.c_float]
+    lib = abi.lib()
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(-10, 10, 3000), rng.normal(0, 1e3, 1000), [0.0, -0.0, 1e-30, 1.0, -1.0]])
+    ys = np.concatenate([rng.uniform(-10, 10, 3000), rng.normal(0, 1e3, 1000), [0.0, 1.0, -2.0, 0.5, 3.0]])
+    def bits(v):
+        return np.float32(v).view(np.uint32)
+    for x, y in zip(xs.astype(np.float32), ys.astype(np.float32)):
+        assert bits(lib.rg_ucrt_sinf(x)) == bits(L.orc_ucrt_sinf(x)), x
+        assert bits(lib.rg_ucrt_cosf(x)) == bits(L.orc_ucrt_cosf(x)), x
+        assert bits(lib.rg_ucrt_atan2f(y, x)) == bits(L.orc_ucrt_atan2f(y, x)), (y, x)
+        ax = abs(x) % 4.0
+        assert bits(lib.rg_ucrt_powf(ax, y)) == bits(L.orc_ucrt_powf(ax, y)), (ax, y)
+
+
+def test_invalid_config_is_rejected_before_any_device_call(arena_mesh):
+    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
+    v, i = arena_mesh
+    with pytest.raises(ValueError):
+        BatchSim(SimConfig(env_count=0), v, i)
+    with pytest.raises(ValueError):
+        BatchSim(SimConfig(env_count=4, max_cars_per_env=9), v, i)
+    with pytest.raises(ValueError):
+        BatchSim(SimConfig(env_count=4), v, i[:-1])
+    bad = v.copy()
+    bad[0, 0] = 12000.0
+    with pytest.raises(ValueError):
+        BatchSim(SimConfig(env_count=4), bad, i)
