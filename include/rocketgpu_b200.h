@@ -232,6 +232,13 @@ RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream);
 /* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
 
+/* The arena tables rg_batch_create builds from a layout, for inspection: per triangle (caller order) 16 floats
+ * a, b, c, normal (Bullet units, uu / 50), the three internal-edge angles and the edge flags (as a float), and the
+ * BVH leaf order (caller triangle index of each leaf in the order queries visit them). Host only. Returns the
+ * triangle count (tables written up to `cap` triangles) or -1 on error (rg_last_error). */
+RG_API int64_t rg_arena_mesh_tables(const rg_arena_layout* layout, float* out_tri16, int32_t* out_leaf_order,
+                                    int64_t cap);
+
 /* The reference's single-precision transcendental routines as the tick evaluates them (reference
  * include/rocketgpu/detail/math.hpp:39-457: UCRT-compatible sinf, cosf, atan2f, powf), for host code that must
  * reproduce the tick's arithmetic (e.g. a config's cached drag factor). */

@@ -18,6 +18,7 @@ EXPORTS = [
     "rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
     "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_step", "rg_batch_synchronize",
     "rg_batch_device_view", "rg_ucrt_sinf", "rg_ucrt_cosf", "rg_ucrt_atan2f", "rg_ucrt_powf",
+    "rg_arena_mesh_tables",
 ]
 
 
@@ -81,5 +82,7 @@ def lib():
         for n in ("rg_ucrt_atan2f", "rg_ucrt_powf"):
             getattr(L, n).argtypes = [ctypes.c_float, ctypes.c_float]
             getattr(L, n).restype = ctypes.c_float
+        L.rg_arena_mesh_tables.argtypes = [vp, vp, vp, i64]
+        L.rg_arena_mesh_tables.restype = i64
         _lib = L
     return _lib

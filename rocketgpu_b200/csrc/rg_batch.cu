@@ -78,6 +78,7 @@ struct rg_batch {
     DeviceArray<rg::BallState> balls;
     DeviceArray<rg::EnvState> envs;
     DeviceArray<int32_t> env_car_count;
+    DeviceArray<rg::BallWorldScratch> ball_world;
     rg::MeshHost mesh_host;
     rg::MeshDevice mesh;
     std::vector<int32_t> host_car_count;
@@ -127,6 +128,7 @@ struct TickArgs {
     rg::BallState* balls;
     rg::EnvState* envs;
     const int32_t* env_car_count;
+    rg::BallWorldScratch* ball_world;
     int32_t env_count;
     rg::TickConfig tc;
     rg::MeshDevice mesh;
@@ -137,11 +139,13 @@ __global__ void __launch_bounds__(128) tick_kernel(TickArgs a, int ticks) {
     if (e >= a.env_count) return;
     rg::BallState b = a.balls[e];
     rg::EnvState env = a.envs[e];
+    rg::BallWorldScratch s = a.ball_world[e];
     for (int t = 0; t < ticks; ++t) {
-        rg::arena_tick(env, b, a.tc, a.mesh);
+        rg::arena_tick(env, b, s, a.tc, a.mesh);
     }
     a.balls[e] = b;
     a.envs[e] = env;
+    a.ball_world[e] = s;
 }
 
 void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
@@ -149,6 +153,7 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
     a.balls = b->balls.ptr;
     a.envs = b->envs.ptr;
     a.env_car_count = b->env_car_count.ptr;
+    a.ball_world = b->ball_world.ptr;
     a.env_count = b->env_count;
     a.tc = b->tc;
     a.mesh = b->mesh;
@@ -255,6 +260,8 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         b->balls.alloc(b->env_count);
         b->envs.alloc(b->env_count);
         b->env_car_count.alloc(b->env_count);
+        b->ball_world.alloc(b->env_count);
+        check(cudaMemset(b->ball_world.ptr, 0, b->env_count * sizeof(rg::BallWorldScratch)), "clear ball manifolds");
         std::vector<rg_ball_state> balls(b->env_count);
         std::vector<rg_env_state> envs(b->env_count);
         for (auto& x : balls) rg_default_ball_state(&x);
@@ -379,6 +386,26 @@ RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
         DeviceGuard dg(b->device);
         check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
     });
+}
+
+RG_API int64_t rg_arena_mesh_tables(const rg_arena_layout* layout, float* out_tri16, int32_t* out_leaf_order,
+                                    int64_t cap) {
+    int64_t n = -1;
+    const int rc = guard([&] {
+        if (!layout) throw std::invalid_argument("null layout");
+        const rg::MeshHost h = rg::build_mesh_host(layout->vertices_uu, layout->vertex_count, layout->indices,
+                                                   layout->index_count);
+        n = static_cast<int64_t>(h.tris.size());
+        for (int64_t t = 0; t < n && t < cap; ++t) {
+            const rg::HostTri& r = h.tris[t];
+            const float f[16] = {r.a.x, r.a.y, r.a.z, r.b.x, r.b.y, r.b.z, r.c.x, r.c.y, r.c.z, r.normal.x,
+                                 r.normal.y, r.normal.z, r.edge_angle[0], r.edge_angle[1], r.edge_angle[2],
+                                 static_cast<float>(r.edge_flags)};
+            if (out_tri16) std::memcpy(out_tri16 + 16 * t, f, sizeof(f));
+            if (out_leaf_order) out_leaf_order[t] = h.leaf_order[t];
+        }
+    });
+    return rc == 0 ? n : -1;
 }
 
 RG_API float rg_ucrt_sinf(float x) { return rg::game_sinf(x); }

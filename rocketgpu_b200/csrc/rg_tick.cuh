@@ -7,6 +7,7 @@
 // (env_step.hpp:4622-5623) and StepEnvTail (env_step.hpp:6968-7045).
 #pragma once
 
+#include "rg_ball_world.cuh"
 #include "rg_math.cuh"
 #include "rg_mesh.h"
 #include "rg_state.cuh"
@@ -171,15 +172,58 @@ RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c) {
 
 // World step, ball-only arena (reference WorldStepSoccar with count == 0, env_step.hpp:4727-5623): activation,
 // arena contacts, gravity, integration and Bullet's deactivation timer.
-RG_HDI void ball_world_step(BallState& b, const TickConfig& c, const MeshDevice& mesh) {
+RG_HDI void ball_world_step(BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& mesh) {
     const float sub_dt = c.tick_dt;  // one world substep per tick
     const bool vehicle_woke = (b.sleeping & 4u) != 0;
     b.sleeping &= 3u;
     const bool ball_sleeping = ball_resolve_activation(b);
     if (vehicle_woke) b.deactivation_time = 0.0f;
     const V3 ext_delta = ball_sleeping ? V3{0.0f, 0.0f, 0.0f} : V3{0.0f, 0.0f, c.gravity_z * sub_dt};
-    (void)mesh;
+    const V3 solver_vel_bt = b.vel_bt;
     const bool awake = !ball_sleeping || vehicle_woke;
+    // predictive contact of this tick's motion (reference ComputePredictiveContactHits, env_step.hpp:4129-4168)
+    V3 pred_n{0, 0, 0};
+    float pred_dist = 0.0f;
+    const bool pred_hit = !(ball_sleeping && !vehicle_woke) && ball_predictive_hit(b, mesh, sub_dt, pred_n, pred_dist);
+    // the persistent manifold list: last tick's predictive entry leaves, a new one is appended, the ball/mesh pair
+    // enters once the ball is awake (reference BuildBulletManifoldList, arena_geometry.hpp:4864-4930)
+    for (int k = 0; k < s.list_count; ++k) {
+        if (s.list[k] == kListPredictive) {
+            s.list[k] = s.list[--s.list_count];
+            break;
+        }
+    }
+    if (pred_hit) s.list[s.list_count++] = kListPredictive;
+    {
+        bool has_mesh = false;
+        for (int k = 0; k < s.list_count; ++k) has_mesh = has_mesh || s.list[k] == kListMesh;
+        if (!has_mesh && !(ball_sleeping && !vehicle_woke)) s.list[s.list_count++] = kListMesh;
+    }
+    // island sort of the listed manifolds: two entries of the ball's island come out reversed (reference
+    // SortBulletManifoldListByIsland, env_step.hpp:4269-4285)
+    int32_t sorted_ids[2];
+    const int n_sorted = s.list_count;
+    for (int k = 0; k < n_sorted; ++k) {
+        const uint8_t e = n_sorted == 2 ? s.list[1 - k] : s.list[k];
+        sorted_ids[k] = e == kListPredictive ? kPredictiveStaticId : 0;
+    }
+    bool pred_listed = false;
+    for (int k = 0; k < n_sorted; ++k) pred_listed = pred_listed || sorted_ids[k] == kPredictiveStaticId;
+    // arena contacts: a sleeping ball keeps its manifold untouched
+    BallContactRows rows;
+    rows.split_count = rows.vel_count = rows.fric_count = 0;
+    if (awake) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
+    if (pred_hit) ball_predictive_rows(b, c, pred_n, pred_dist, ext_delta, solver_vel_bt, sub_dt, rows);
+    if (rows.vel_count || rows.fric_count) {
+        V3 dl, da;
+        ball_solve_velocity(rows, pred_listed, dl, da);
+        ball_set_vel_bt(b, solver_vel_bt + dl);
+        b.ang_vel = b.ang_vel + da;
+    }
+    if (rows.split_count) {
+        const V3 push = ball_solve_split(rows, sorted_ids, n_sorted);
+        if (!is_zero(push)) ball_set_pos_bt(b, b.pos_bt + push * sub_dt);
+    }
     if (!ball_sleeping) ball_set_vel_bt(b, b.vel_bt + uu_to_bt_div(ext_delta));
     if (awake) {
         ball_integrate(b, sub_dt);
@@ -191,11 +235,12 @@ RG_HDI void ball_world_step(BallState& b, const TickConfig& c, const MeshDevice&
 }
 
 // One tick of one ball-only arena (reference StepEnvGeneric, env_step.hpp:7088-7180).
-RG_HDI void arena_tick(EnvState& env, BallState& b, const TickConfig& c, const MeshDevice& mesh) {
+RG_HDI void arena_tick(EnvState& env, BallState& b, BallWorldScratch& s, const TickConfig& c,
+                       const MeshDevice& mesh) {
     env.goal_scored_this_tick = 0;
     ball_tick_start_quantize(b, c);
     ball_clamp_and_drag(b, c);
-    ball_world_step(b, c, mesh);
+    ball_world_step(b, s, c, mesh);
     env_tail(env, b, c);
 }
 

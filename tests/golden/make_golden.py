@@ -40,3 +40,4 @@ def run_ball_case(name: str, states_fn, n: int, seed: int, ticks: int):
 
 if __name__ == "__main__":
     run_ball_case("ball_free_flight", scenarios.free_flight_states, 8, 1234, 60)
+    run_ball_case("ball_contacts", scenarios.ball_states, 8, 4321, 200)

@@ -84,3 +84,53 @@ def test_golden_free_flight(arena_mesh):
         gpu.step(1)
         assert bytes(gpu.download_ball_states()) == bytes(g["balls"][t]), t
         assert bytes(gpu.download_env_states()) == bytes(g["envs"][t]), t
+
+
+def test_contact_heavy_parity_every_tick(oracle_available, arena_mesh):
+    """Balls thrown at up to 6000 uu/s: bounces, rolling, corner and edge contacts, predictive (CCD) contacts."""
+    n = 1024
+    orc, gpu = _pair(n, arena_mesh)
+    _, default_ball, _, _, _ = oracle_ref.default_states()
+    init = scenarios.ball_states(default_ball, n, seed=21)
+    orc.upload_balls(init)
+    gpu.upload_ball_states(init)
+    gpu.upload_env_states(orc.envs())
+    for t in range(600):
+        orc.step(1)
+        gpu.step(1)
+        d = _first_diff(orc.balls(), gpu.download_ball_states())
+        assert d is None, f"tick {t}: ball {d}"
+        d = _first_diff(orc.envs(), gpu.download_env_states())
+        assert d is None, f"tick {t}: env {d}"
+
+
+def test_contact_heavy_multi_tick_launches(oracle_available, arena_mesh):
+    n = 2048
+    orc, gpu = _pair(n, arena_mesh)
+    _, default_ball, _, _, _ = oracle_ref.default_states()
+    init = scenarios.ball_states(default_ball, n, seed=22)
+    orc.upload_balls(init)
+    gpu.upload_ball_states(init)
+    gpu.upload_env_states(orc.envs())
+    for k in range(100):
+        orc.step(8)
+        gpu.step(8)
+        d = _first_diff(orc.balls(), gpu.download_ball_states())
+        assert d is None, f"launch {k}: ball {d}"
+        d = _first_diff(orc.envs(), gpu.download_env_states())
+        assert d is None, f"launch {k}: env {d}"
+
+
+def test_golden_contacts(arena_mesh):
+    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
+    g = np.load(os.path.join(HERE, "golden", "ball_contacts.npz"))
+    v, i = arena_mesh
+    n = g["init_balls"].shape[0]
+    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=2), v, i)
+    gpu.set_env_car_count([0] * n)
+    gpu.upload_ball_states(g["init_balls"])
+    gpu.upload_env_states(g["init_envs"])
+    for t in range(g["balls"].shape[0]):
+        gpu.step(1)
+        assert bytes(gpu.download_ball_states()) == bytes(g["balls"][t]), t
+        assert bytes(gpu.download_env_states()) == bytes(g["envs"][t]), t

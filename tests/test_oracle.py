@@ -34,3 +34,48 @@ def test_oracle_reproduces_golden_free_flight(oracle_available, arena_mesh):
         sim.step(1)
         assert bytes(sim.balls()) == bytes(g["balls"][t]), t
         assert bytes(sim.envs()) == bytes(g["envs"][t]), t
+
+
+def test_oracle_reproduces_golden_contacts(oracle_available, arena_mesh):
+    g = np.load(os.path.join(HERE, "golden", "ball_contacts.npz"))
+    v, i = arena_mesh
+    n = g["init_balls"].shape[0]
+    sim = oracle_ref.OracleSim(n, 2, v, i, kickoff_settled=False)
+    sim.set_env_car_count([0] * n)
+    _, default_ball, _, _, _ = oracle_ref.default_states()
+    init = scenarios.ball_states(default_ball, n, int(g["seed"]))
+    assert bytes(init) == bytes(g["init_balls"])
+    sim.upload_balls(init)
+    for t in range(g["balls"].shape[0]):
+        sim.step(1)
+        assert bytes(sim.balls()) == bytes(g["balls"][t]), t
+
+
+def test_mesh_tables_match_reference(oracle_available, arena_mesh):
+    """The product's arena build (triangles, internal-edge angles, BVH leaf order) equals the reference loader's."""
+    import ctypes
+
+    from rocketgpu_b200 import abi, arena
+    L = oracle_ref.lib()
+    L.orc_mesh_tables.restype = ctypes.c_int64
+    L.orc_mesh_tables.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_void_p, ctypes.c_int64]
+    L.orc_mesh_nodes.restype = ctypes.c_int64
+    L.orc_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+    for v, i in (arena_mesh, arena.generate_dense()):
+        nt = len(i) // 3
+        ref = np.zeros((nt, 16), np.float32)
+        assert L.orc_mesh_tables(v.ctypes.data, len(v), i.ctypes.data, len(i), ref.ctypes.data, nt) == nt
+        nodes = np.zeros((2 * nt, 7), np.int32)
+        nn = L.orc_mesh_nodes(nodes.ctypes.data, 2 * nt)
+        ref_leaf = nodes[:nn][nodes[:nn, 6] >= 0, 6]
+        lay = abi.rg_arena_layout()
+        lay.vertices_uu = v.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        lay.vertex_count = len(v)
+        lay.indices = i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        lay.index_count = len(i)
+        mine = np.zeros((nt, 16), np.float32)
+        leaf = np.zeros(nt, np.int32)
+        assert abi.lib().rg_arena_mesh_tables(ctypes.byref(lay), mine.ctypes.data, leaf.ctypes.data, nt) == nt
+        assert bytes(mine) == bytes(ref)
+        assert (leaf == ref_leaf).all()
