@@ -255,6 +255,25 @@ typedef struct rg_device_view {
 } rg_device_view;
 RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
 
+/* Steps ball-only arenas whose states live in caller-owned device memory, without allocating any device memory.
+ * No counterpart in the reference: an addition of this library.
+ *
+ * For callers that cannot call cudaMalloc when they step: a process whose device memory is owned by another
+ * framework's pool, a loop that must not pay the implicit synchronisation an allocation can cause, or code stepping
+ * while someone else captures a stream. The batch `b` (created beforehand, when allocation was allowed) supplies
+ * the arena mesh and the config; dev_balls / dev_envs (rg_ball_state[env_count], rg_env_state[env_count], device
+ * pointers, updated in place) are the arenas stepped, `ticks` ticks each, on `stream`.
+ *
+ * The contact manifolds the tick keeps between ticks go to one fixed array compiled into the library (capacity 4096
+ * arenas, about 1.1 MB, held on every GPU that loads the library until the process exits); env_count above 4096 is
+ * rejected (status 3). All calls share that array and it keeps what the last call left: reset_manifolds != 0 clears
+ * the first env_count entries before stepping (do so whenever these arenas were not the ones stepped last); 0
+ * continues from the previous call's manifolds. Calls that overlap on the GPU race on the array: serialise them
+ * (one stream, or events). The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture. */
+RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, rg_env_state* dev_envs,
+                                        int32_t env_count, int32_t ticks, int32_t reset_manifolds, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

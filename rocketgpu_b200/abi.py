@@ -18,7 +18,7 @@ EXPORTS = [
     "rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
     "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_step", "rg_batch_synchronize",
     "rg_batch_device_view", "rg_ucrt_sinf", "rg_ucrt_cosf", "rg_ucrt_atan2f", "rg_ucrt_powf",
-    "rg_arena_mesh_tables",
+    "rg_arena_mesh_tables", "rg_batch_step_static_scratch",
 ]
 
 
@@ -84,5 +84,6 @@ def lib():
             getattr(L, n).restype = ctypes.c_float
         L.rg_arena_mesh_tables.argtypes = [vp, vp, vp, i64]
         L.rg_arena_mesh_tables.restype = i64
+        L.rg_batch_step_static_scratch.argtypes = [vp, vp, vp, i32, i32, i32, vp]
         _lib = L
     return _lib

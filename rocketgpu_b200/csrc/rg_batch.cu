@@ -423,3 +423,67 @@ RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Stepping without any device allocation.
+//
+// The per-arena contact manifolds a tick keeps between ticks normally live in memory rg_batch_create allocates, one
+// entry per arena of the batch. For callers that may not allocate device memory at the point where they step (a
+// process whose device memory belongs to another framework's pool, code that must not trigger the implicit
+// synchronisation cudaMalloc can cause, or a step recorded while some other code is capturing a stream), this entry
+// point keeps those manifolds in one fixed array compiled into the library instead. The array is a file-scope
+// __device__ variable, so every GPU that loads the library holds it (kStaticScratchEnvs entries of
+// sizeof(rg::BallWorldScratch) bytes, about 1.1 MB) until the process exits.
+namespace {
+constexpr int kStaticScratchEnvs = 4096;
+static __device__ __align__(256) rg::BallWorldScratch g_static_ball_world[kStaticScratchEnvs];
+
+constexpr int kMaxDevices = 64;
+void* g_static_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_static_ball_world on the current device. In host code the symbol's name stands for a host-side
+// shadow, not the device array, so the address comes from cudaGetSymbolAddress, once per device.
+rg::BallWorldScratch* static_scratch_address(int device) {
+    if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device index out of range");
+    if (g_static_scratch_addr[device] == nullptr) {
+        void* p = nullptr;
+        check(cudaGetSymbolAddress(&p, g_static_ball_world), "cudaGetSymbolAddress(static scratch)");
+        g_static_scratch_addr[device] = p;
+    }
+    return static_cast<rg::BallWorldScratch*>(g_static_scratch_addr[device]);
+}
+}  // namespace
+
+extern "C" {
+
+RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, rg_env_state* dev_envs,
+                                        int32_t env_count, int32_t ticks, int32_t reset_manifolds, void* stream) {
+    return guard([&] {
+        if (!b || !dev_balls || !dev_envs) throw std::invalid_argument("null argument");
+        if (env_count <= 0) throw std::invalid_argument("env_count must be positive");
+        if (env_count > kStaticScratchEnvs)
+            throw std::out_of_range("env_count exceeds the static scratch capacity (4096 arenas)");
+        if (ticks < 0) throw std::invalid_argument("ticks must be >= 0");
+        DeviceGuard dg(b->device);
+        rg::BallWorldScratch* scratch = static_scratch_address(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (reset_manifolds) {
+            check(cudaMemsetAsync(scratch, 0, static_cast<size_t>(env_count) * sizeof(rg::BallWorldScratch), s),
+                  "clear static scratch");
+        }
+        if (ticks == 0) return;
+        TickArgs a;
+        a.balls = reinterpret_cast<rg::BallState*>(dev_balls);
+        a.envs = reinterpret_cast<rg::EnvState*>(dev_envs);
+        a.env_car_count = b->env_car_count.ptr;
+        a.ball_world = scratch;
+        a.env_count = env_count;
+        a.tc = b->tc;
+        a.mesh = b->mesh;
+        const int threads = 128;
+        tick_kernel<<<(env_count + threads - 1) / threads, threads, 0, s>>>(a, ticks);
+        check(cudaGetLastError(), "tick_kernel launch (static scratch)");
+    });
+}
+
+}  // extern "C"
