@@ -561,7 +561,7 @@ RG_HDI void mesh_query_box(const MeshDevice& m, V3 lo, V3 hi, F&& visit) {
     const bool small = (hi.x - lo.x) <= kQueryExtentBt && (hi.y - lo.y) <= kQueryExtentBt &&
                        (hi.z - lo.z) <= kQueryExtentBt;
     int begin = 0, end = m.tri_count;
-    const int32_t* list = nullptr;
+    const CellEntry* list = m.rank_entries;
     if (small) {
         int cell[3];
         for (int a = 0; a < 3; ++a) {
@@ -572,15 +572,28 @@ RG_HDI void mesh_query_box(const MeshDevice& m, V3 lo, V3 hi, F&& visit) {
         const int ci = (cell[2] * m.grid_dims[1] + cell[1]) * m.grid_dims[0] + cell[0];
         begin = m.cell_start[ci];
         end = m.cell_start[ci + 1];
-        list = m.cell_tris;
+        list = m.cell_entries;
     }
-    for (int e = begin; e < end; ++e) {
-        const int r = list ? list[e] : e;
-        const DevTri& t = m.tris[r];
-        if (qmin[0] > t.qmax[0] || qmax[0] < t.qmin[0] || qmin[1] > t.qmax[1] || qmax[1] < t.qmin[1] ||
-            qmin[2] > t.qmax[2] || qmax[2] < t.qmin[2])
-            continue;
-        visit(t);
+    // entries are tested four at a time: the four 16-byte loads are independent, so their latencies overlap
+    auto overlaps = [&](const CellEntry& t) {
+        return !(qmin[0] > t.qmax[0] || qmax[0] < t.qmin[0] || qmin[1] > t.qmax[1] || qmax[1] < t.qmin[1] ||
+                 qmin[2] > t.qmax[2] || qmax[2] < t.qmin[2]);
+    };
+    for (int e = begin; e < end; e += 4) {
+        int rank[4];
+        unsigned hits = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const CellEntry en = list[e + k < end ? e + k : e];
+            rank[k] = en.rank;
+            hits |= (e + k < end && overlaps(en)) ? (1u << k) : 0u;
+        }
+        while (hits != 0u) {
+            const int k = ctz32(hits);
+            hits &= hits - 1u;
+            const int r = k == 0 ? rank[0] : (k == 1 ? rank[1] : (k == 2 ? rank[2] : rank[3]));
+            visit(m.tris[r]);
+        }
     }
 }
 

@@ -3,8 +3,8 @@
 // Execution model. One CUDA thread owns one arena for the whole launch: it loads the arena's ball and env state from
 // HBM once, runs `ticks` ticks with the state in registers, and stores it back once. Arenas are independent (the
 // reference steps each env in isolation, include/rocketgpu/detail/step/env_step.hpp:7048), so a step is one launch
-// over ceil(envs / 128) blocks with no inter-thread communication; at 16K arenas that is ~128 blocks, under one wave
-// of the 148 SMs. Ticks per launch amortise the state load/store and launch latency.
+// of single-warp blocks with no inter-thread communication; at 16K arenas that is 512 blocks, about 3.5 per SM on the
+// 148 SMs. Ticks per launch amortise the state load/store and launch latency.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -82,6 +82,7 @@ struct rg_batch {
     rg::MeshHost mesh_host;
     rg::MeshDevice mesh;
     std::vector<int32_t> host_car_count;
+    int launch_threads = 32;
 };
 
 namespace {
@@ -134,7 +135,7 @@ struct TickArgs {
     rg::MeshDevice mesh;
 };
 
-__global__ void __launch_bounds__(128) tick_kernel(TickArgs a, int ticks) {
+__global__ void __launch_bounds__(32) tick_kernel(TickArgs a, int ticks) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.env_count) return;
     rg::BallState b = a.balls[e];
@@ -157,7 +158,9 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
     a.env_count = b->env_count;
     a.tc = b->tc;
     a.mesh = b->mesh;
-    const int threads = 128;
+    // One warp per block: an arena is one thread, so 16K arenas are only 512 warps; single-warp blocks spread them
+    // over all 148 SMs (128-thread blocks left 20 SMs idle at 16K arenas).
+    const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
     tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
     check(cudaGetLastError(), "tick_kernel launch");
@@ -480,7 +483,7 @@ RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, r
         a.env_count = env_count;
         a.tc = b->tc;
         a.mesh = b->mesh;
-        const int threads = 128;
+        const int threads = b->launch_threads;
         tick_kernel<<<(env_count + threads - 1) / threads, threads, 0, s>>>(a, ticks);
         check(cudaGetLastError(), "tick_kernel launch (static scratch)");
     });

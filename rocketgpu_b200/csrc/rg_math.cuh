@@ -54,6 +54,15 @@ RG_HD V3 vmax(V3 a, V3 b) { return V3{fmax_(a.x, b.x), fmax_(a.y, b.y), fmax_(a.
 RG_HD float div50(float x) { return x / 50.0f; }
 RG_HD V3 uu_to_bt_div(V3 v) { return V3{div50(v.x), div50(v.y), div50(v.z)}; }
 
+// Index of the lowest set bit (x != 0).
+RG_HD int ctz32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __ffs(static_cast<int>(x)) - 1;
+#else
+    return __builtin_ctz(x);
+#endif
+}
+
 RG_HD uint32_t f2u(float f) {
     uint32_t u;
     memcpy(&u, &f, 4);

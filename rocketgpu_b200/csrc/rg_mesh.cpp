@@ -355,8 +355,20 @@ MeshHost build_mesh_host(const float* v, int64_t nv, const int32_t* idx, int64_t
     }
     h.cell_start.assign(static_cast<size_t>(cells) + 1, 0);
     for (int64_t c = 0; c < cells; ++c) h.cell_start[c + 1] = h.cell_start[c] + static_cast<int32_t>(lists[c].size());
-    h.cell_tris.reserve(static_cast<size_t>(h.cell_start[cells]));
-    for (auto& l : lists) h.cell_tris.insert(h.cell_tris.end(), l.begin(), l.end());
+    auto entry_of = [&](int32_t r) {
+        CellEntry e;
+        for (int a = 0; a < 3; ++a) {
+            e.qmin[a] = h.dev_tris[r].qmin[a];
+            e.qmax[a] = h.dev_tris[r].qmax[a];
+        }
+        e.rank = r;
+        return e;
+    };
+    h.cell_entries.reserve(static_cast<size_t>(h.cell_start[cells]));
+    for (auto& l : lists)
+        for (int32_t r : l) h.cell_entries.push_back(entry_of(r));
+    h.rank_entries.reserve(static_cast<size_t>(nt));
+    for (int32_t r = 0; r < nt; ++r) h.rank_entries.push_back(entry_of(r));
     return h;
 }
 
@@ -388,14 +400,16 @@ MeshDevice upload_mesh(const MeshHost& h) {
     d.grid_lo = h.grid_lo;
     for (int a = 0; a < 3; ++a) d.grid_dims[a] = h.grid_dims[a];
     d.cell_start = upload_array(h.cell_start, "mesh grid");
-    d.cell_tris = upload_array(h.cell_tris, "mesh grid lists");
+    d.cell_entries = upload_array(h.cell_entries, "mesh grid lists");
+    d.rank_entries = upload_array(h.rank_entries, "mesh rank list");
     return d;
 }
 
 void free_mesh(MeshDevice& d) {
     if (d.tris) cudaFree(const_cast<DevTri*>(d.tris));
     if (d.cell_start) cudaFree(const_cast<int32_t*>(d.cell_start));
-    if (d.cell_tris) cudaFree(const_cast<int32_t*>(d.cell_tris));
+    if (d.cell_entries) cudaFree(const_cast<CellEntry*>(d.cell_entries));
+    if (d.rank_entries) cudaFree(const_cast<CellEntry*>(d.rank_entries));
     d = MeshDevice{};
 }
 

@@ -47,6 +47,13 @@ struct HostTri {
 constexpr float kQueryCellBt = 4.0f;
 constexpr float kQueryExtentBt = 4.0f;
 
+// One query-grid entry: a triangle's quantized leaf bounds and its rank, so the overlap test needs no triangle load.
+struct alignas(16) CellEntry {
+    uint16_t qmin[3], qmax[3];
+    int32_t rank;
+};
+static_assert(sizeof(CellEntry) == 16, "CellEntry is one 16-byte word");
+
 struct MeshHost {
     std::vector<HostTri> tris;          // caller order
     std::vector<int32_t> leaf_order;    // BVH leaf rank -> caller triangle index
@@ -56,8 +63,9 @@ struct MeshHost {
     // query grid
     V3 grid_lo{0, 0, 0};
     int32_t grid_dims[3] = {0, 0, 0};
-    std::vector<int32_t> cell_start;    // grid cell -> first entry, size cells + 1
-    std::vector<int32_t> cell_tris;     // ranks
+    std::vector<int32_t> cell_start;       // grid cell -> first entry, size cells + 1
+    std::vector<CellEntry> cell_entries;   // per cell, in rank order
+    std::vector<CellEntry> rank_entries;   // every triangle in rank order (queries larger than one cell)
 };
 
 // Device view (plain pointers; lives in the rg_batch).
@@ -69,7 +77,8 @@ struct MeshDevice {
     V3 grid_lo{0, 0, 0};
     int32_t grid_dims[3] = {0, 0, 0};
     const int32_t* cell_start = nullptr;
-    const int32_t* cell_tris = nullptr;
+    const CellEntry* cell_entries = nullptr;
+    const CellEntry* rank_entries = nullptr;
 };
 
 MeshHost build_mesh_host(const float* vertices_uu, int64_t vertex_count, const int32_t* indices, int64_t index_count);
