@@ -35,7 +35,10 @@ ENVS = 16384
 TICKS_PER_STEP = 8
 METRIC = "arena-ticks/s"
 WORKLOAD = "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step"
-STATE_BYTES_PER_ARENA = 288 + 44  # ball + env struct, read and written once per launch
+# dram__bytes_read.sum + dram__bytes_write.sum of one tick_kernel launch at this workload, from the ncu capture
+# summarised in profiles/tick_kernel_ball_arenas_16k.md
+TRAFFIC_PER_LAUNCH = 16.01e6
+STATE_BYTES_PER_ARENA = 288 + 288 + 44  # ball struct + ball contact state + env struct, read and written per launch
 
 
 def peaks():
@@ -196,7 +199,7 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
                    "l2": "256 MiB flush before every timed step", "parallelism": f"arena shards x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_kind, "traffic": None,
+                     "peak_source": peak_kind, "traffic": TRAFFIC_PER_LAUNCH,
                      "note": "state traffic only; the tick is FP32-issue/latency bound, not HBM bound"},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ENVS * 288},
         "gpu_launches": args.steps,
