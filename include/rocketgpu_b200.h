@@ -205,6 +205,9 @@ RG_API void rg_sim_config_default(rg_sim_config* cfg);
 /* Reference-default public states (the reference's member initialisers), for callers building uploads. */
 RG_API void rg_default_ball_state(rg_ball_state* out);
 RG_API void rg_default_env_state(rg_env_state* out);
+/* CarState{} and CarConfig{} (the Octane preset) — reference rocketgpu.h:135-175, 190-502. */
+RG_API void rg_default_car_state(rg_car_state* out);
+RG_API void rg_default_car_config(rg_car_config* out);
 
 /* BatchSim(config, layout) — reference rocketgpu.h:990-992, src/rocketgpu.cpp:1019-1250. Validates the config
  * (env_count > 0, 0 <= max_cars_per_env <= 8) and layout (finite, within 11,500 uu), builds the mesh BVH on the
@@ -224,10 +227,30 @@ RG_API int rg_batch_download_ball_states(rg_batch* b, rg_ball_state* host, size_
 /* BatchSim::upload_env_states / download_env_states (rocketgpu.h:1027,1047). */
 RG_API int rg_batch_upload_env_states(rg_batch* b, const rg_env_state* host, size_t count, void* stream);
 RG_API int rg_batch_download_env_states(rg_batch* b, rg_env_state* host, size_t count, void* stream);
+/* BatchSim::upload_car_states in PublicState mode / download_car_states (rocketgpu.h:1028,1036; src/rocketgpu.cpp:
+ * 2952-2965 with the import canonicalisation of src/rocketgpu.cpp:355-379). Slot j of env e is index
+ * e * max_cars_per_env + j. */
+RG_API int rg_batch_upload_car_states(rg_batch* b, const rg_car_state* host, size_t count, void* stream);
+RG_API int rg_batch_download_car_states(rg_batch* b, rg_car_state* host, size_t count, void* stream);
+/* BatchSim::boost_pad_capacity / upload_boost_pad_states / download_boost_pad_states (rocketgpu.h:1019,1034,1048):
+ * 34 pads per env (the layout's default soccar pads), pad p of env e at index e * 34 + p. */
+RG_API int64_t rg_batch_pad_capacity(const rg_batch* b);
+RG_API int rg_batch_upload_pad_states(rg_batch* b, const rg_boost_pad_state* host, size_t count, void* stream);
+RG_API int rg_batch_download_pad_states(rg_batch* b, rg_boost_pad_state* host, size_t count, void* stream);
+/* BatchSim::set_car_configs (rocketgpu.h:1025). Three-wheel configs are rejected (invalid_argument): that car
+ * model is not built. */
+RG_API int rg_batch_set_car_configs(rg_batch* b, const rg_car_config* host, size_t count, void* stream);
+/* BatchSim::upload_controls (rocketgpu.h:1032): the controls rg_batch_step holds for every tick. */
+RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream);
 
 /* BatchSim::step (rocketgpu.h:1063; src/rocketgpu.cpp:3237): advances every env by `ticks` 120 Hz ticks on `stream`
  * (asynchronous; no host synchronisation). */
 RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream);
+/* BatchSim::step_with_device_controls (rocketgpu.h:1075; checks src/rocketgpu.cpp:2412-2421): tick t reads car i's
+ * controls at device_controls[t * control_stride + i]; control_stride 0 holds one row for every tick, otherwise it
+ * must be at least the car capacity. ticks <= 0 does nothing. */
+RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls* device_controls, int32_t ticks,
+                                              int32_t control_stride, void* stream);
 
 /* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
@@ -252,6 +275,9 @@ typedef struct rg_device_view {
     void* ball_states;       /* rg_ball_state[env_count] */
     void* env_states;        /* rg_env_state[env_count] */
     int32_t* env_car_count;  /* [env_count] */
+    void* car_states;        /* rg_car_state[car_capacity] */
+    void* boost_pad_states;  /* rg_boost_pad_state[pad_capacity] */
+    void* controls;          /* rg_car_controls[car_capacity] */
 } rg_device_view;
 RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
 

@@ -19,6 +19,9 @@ EXPORTS = [
     "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_step", "rg_batch_synchronize",
     "rg_batch_device_view", "rg_ucrt_sinf", "rg_ucrt_cosf", "rg_ucrt_atan2f", "rg_ucrt_powf",
     "rg_arena_mesh_tables", "rg_batch_step_static_scratch",
+    "rg_default_car_state", "rg_default_car_config", "rg_batch_upload_car_states", "rg_batch_download_car_states",
+    "rg_batch_pad_capacity", "rg_batch_upload_pad_states", "rg_batch_download_pad_states", "rg_batch_set_car_configs",
+    "rg_batch_upload_controls", "rg_batch_step_with_device_controls",
 ]
 
 
@@ -45,7 +48,8 @@ class rg_arena_layout(ctypes.Structure):
 
 class rg_device_view(ctypes.Structure):
     _fields_ = [("ball_states", ctypes.c_void_p), ("env_states", ctypes.c_void_p),
-                ("env_car_count", ctypes.c_void_p)]
+                ("env_car_count", ctypes.c_void_p), ("car_states", ctypes.c_void_p),
+                ("boost_pad_states", ctypes.c_void_p), ("controls", ctypes.c_void_p)]
 
 
 _lib = None
@@ -71,7 +75,9 @@ def lib():
         L.rg_batch_car_capacity.argtypes = [vp]
         L.rg_batch_car_capacity.restype = i64
         for n in ("rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
-                  "rg_batch_upload_env_states", "rg_batch_download_env_states"):
+                  "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_upload_car_states",
+                  "rg_batch_download_car_states", "rg_batch_upload_pad_states", "rg_batch_download_pad_states",
+                  "rg_batch_set_car_configs", "rg_batch_upload_controls"):
             getattr(L, n).argtypes = [vp, vp, sz, vp]
         L.rg_batch_step.argtypes = [vp, i32, vp]
         L.rg_batch_synchronize.argtypes = [vp, vp]
@@ -85,5 +91,10 @@ def lib():
         L.rg_arena_mesh_tables.argtypes = [vp, vp, vp, i64]
         L.rg_arena_mesh_tables.restype = i64
         L.rg_batch_step_static_scratch.argtypes = [vp, vp, vp, i32, i32, i32, vp]
+        L.rg_default_car_state.argtypes = [vp]
+        L.rg_default_car_config.argtypes = [vp]
+        L.rg_batch_pad_capacity.argtypes = [vp]
+        L.rg_batch_pad_capacity.restype = i64
+        L.rg_batch_step_with_device_controls.argtypes = [vp, vp, i32, i32, vp]
         _lib = L
     return _lib

@@ -15,7 +15,7 @@ import numpy as np
 
 from . import abi
 
-CAR_BYTES, BALL_BYTES, ENV_BYTES = 880, 288, 44
+CAR_BYTES, BALL_BYTES, ENV_BYTES, PAD_BYTES, CONTROLS_BYTES, CAR_CONFIG_BYTES = 880, 288, 44, 16, 24, 120
 
 
 def _check(rc: int):
@@ -108,6 +108,42 @@ class BatchSim:
         _check(abi.lib().rg_batch_download_env_states(self._h, _ptr(out), n, stream))
         return out
 
+    def pad_capacity(self) -> int:
+        return abi.lib().rg_batch_pad_capacity(self._h)
+
+    def upload_car_states(self, states: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(states, np.uint8).reshape(-1, CAR_BYTES)
+        _check(abi.lib().rg_batch_upload_car_states(self._h, _ptr(s), len(s), stream))
+
+    def download_car_states(self, count: int | None = None, stream: int = 0) -> np.ndarray:
+        n = self.car_capacity() if count is None else count
+        out = np.zeros((n, CAR_BYTES), np.uint8)
+        _check(abi.lib().rg_batch_download_car_states(self._h, _ptr(out), n, stream))
+        return out
+
+    def upload_boost_pad_states(self, states: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(states, np.uint8).reshape(-1, PAD_BYTES)
+        _check(abi.lib().rg_batch_upload_pad_states(self._h, _ptr(s), len(s), stream))
+
+    def download_boost_pad_states(self, count: int | None = None, stream: int = 0) -> np.ndarray:
+        n = self.pad_capacity() if count is None else count
+        out = np.zeros((n, PAD_BYTES), np.uint8)
+        _check(abi.lib().rg_batch_download_pad_states(self._h, _ptr(out), n, stream))
+        return out
+
+    def set_car_configs(self, configs: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(configs, np.uint8).reshape(-1, CAR_CONFIG_BYTES)
+        _check(abi.lib().rg_batch_set_car_configs(self._h, _ptr(s), len(s), stream))
+
+    def upload_controls(self, controls: np.ndarray, stream: int = 0):
+        s = np.ascontiguousarray(controls, np.uint8).reshape(-1, CONTROLS_BYTES)
+        _check(abi.lib().rg_batch_upload_controls(self._h, _ptr(s), len(s), stream))
+
+    def step_with_device_controls(self, device_controls: int, ticks: int, control_stride: int, stream: int = 0):
+        """`device_controls` is a device pointer to rg_car_controls rows (e.g. a torch uint8 tensor's data_ptr())."""
+        _check(abi.lib().rg_batch_step_with_device_controls(self._h, ctypes.c_void_p(device_controls), ticks,
+                                                            control_stride, stream))
+
     def step(self, ticks: int = 1, stream: int = 0):
         _check(abi.lib().rg_batch_step(self._h, ticks, stream))
 
@@ -117,4 +153,5 @@ class BatchSim:
     def device_view(self) -> dict:
         v = abi.rg_device_view()
         _check(abi.lib().rg_batch_device_view(self._h, ctypes.byref(v)))
-        return {"ball_states": v.ball_states, "env_states": v.env_states, "env_car_count": v.env_car_count}
+        return {"ball_states": v.ball_states, "env_states": v.env_states, "env_car_count": v.env_car_count,
+                "car_states": v.car_states, "boost_pad_states": v.boost_pad_states, "controls": v.controls}

@@ -597,6 +597,43 @@ RG_HDI void mesh_query_box(const MeshDevice& m, V3 lo, V3 hi, F&& visit) {
     }
 }
 
+// Bullet's ray-vs-leaf-box test of the quantized BVH walk: the ray must cross the leaf's dequantized bounds within its
+// length (reference ArenaMeshBvhRayLeaf, include/rocketgpu/detail/arena/mesh_bvh.hpp:522-558, and the same slab test
+// in HostRayCastArenaMeshBlocks, host_validation_and_contact_debug.hpp:1591-1602).
+struct RayLeaf {
+    V3 src, inv;
+    float lambda_max;
+};
+RG_HDI RayLeaf make_ray_leaf(V3 from, V3 to) {
+    RayLeaf r;
+    const V3 d = to - from;
+    const float rl = 1.0f / sqrtf(d.y * d.y + d.x * d.x + d.z * d.z);
+    const V3 n{d.x * rl, d.y * rl, d.z * rl};
+    r.lambda_max = n.x * d.x + n.y * d.y + n.z * d.z;
+    r.inv = V3{n.x == 0.0f ? 1e18f : 1.0f / n.x, n.y == 0.0f ? 1e18f : 1.0f / n.y, n.z == 0.0f ? 1e18f : 1.0f / n.z};
+    r.src = from;
+    return r;
+}
+RG_HDI bool ray_leaf_hits(const Quantization& q, const RayLeaf& r, const uint16_t* qmin, const uint16_t* qmax) {
+    const V3 lo{q.aabb_min.x + static_cast<float>(qmin[0]) / q.scale.x,
+                q.aabb_min.y + static_cast<float>(qmin[1]) / q.scale.y,
+                q.aabb_min.z + static_cast<float>(qmin[2]) / q.scale.z};
+    const V3 hi{q.aabb_min.x + static_cast<float>(qmax[0]) / q.scale.x,
+                q.aabb_min.y + static_cast<float>(qmax[1]) / q.scale.y,
+                q.aabb_min.z + static_cast<float>(qmax[2]) / q.scale.z};
+    const float tmin = ((r.inv.x < 0.0f ? hi.x : lo.x) - r.src.x) * r.inv.x;
+    const float tmax = ((r.inv.x < 0.0f ? lo.x : hi.x) - r.src.x) * r.inv.x;
+    const float tymin = ((r.inv.y < 0.0f ? hi.y : lo.y) - r.src.y) * r.inv.y;
+    const float tymax = ((r.inv.y < 0.0f ? lo.y : hi.y) - r.src.y) * r.inv.y;
+    if (!(tmin <= tymax) || !(tymin <= tmax)) return false;
+    const float t0 = tymin <= tmin ? tmin : tymin;
+    const float t1 = tmax <= tymax ? tmax : tymax;
+    const float tzmin = ((r.inv.z < 0.0f ? hi.z : lo.z) - r.src.z) * r.inv.z;
+    const float tzmax = ((r.inv.z < 0.0f ? lo.z : hi.z) - r.src.z) * r.inv.z;
+    if (!(t0 <= tzmax) || !(tzmin <= t1)) return false;
+    return (tzmin <= t0 ? t0 : tzmin) < r.lambda_max && 0.0f < (t1 <= tzmax ? t1 : tzmax);
+}
+
 // Closest hit of the segment from -> to against the mesh, Bullet's triangle ray test in the reference's arithmetic
 // (btTriangleRaycastCallback as evaluated by HostRayCastArenaMeshBlocks, host_validation_and_contact_debug.hpp:
 // 1603-1690): returns the hit fraction and the hit triangle, ties kept by the first triangle in leaf order.
@@ -605,7 +642,9 @@ RG_HDI bool mesh_ray_closest(const MeshDevice& m, V3 from, V3 to, float& out_fra
     float hit_fraction = 0.0f;
     float fraction = 1.0f;
     const DevTri* win = nullptr;
+    const RayLeaf leaf = make_ray_leaf(from, to);
     mesh_query_box(m, vmin(from, to), vmax(from, to), [&](const DevTri& t) {
+        if (!ray_leaf_hits(m.quant, leaf, t.qmin, t.qmax)) return;
         const V3 n = cross(t.b - t.a, t.c - t.a);
         const float plane = dot(t.a, n);
         const float dist_a = ((n.x * from.x + n.y * from.y) + n.z * from.z) - plane;

@@ -79,6 +79,14 @@ struct rg_batch {
     DeviceArray<rg::EnvState> envs;
     DeviceArray<int32_t> env_car_count;
     DeviceArray<rg::BallWorldScratch> ball_world;
+    DeviceArray<rg::CarState> cars;
+    DeviceArray<rg::WheelRuntime> wheels;
+    DeviceArray<rg::CarConfig> car_cfgs;
+    DeviceArray<rg::CarControls> controls;
+    DeviceArray<rg::PadState> pads;
+    rg::PadLayout pad_layout{};
+    // Pads stay at their initial state until a car exists or pads are uploaded; until then ball-only arenas skip them.
+    bool pads_live = false;
     rg::MeshHost mesh_host;
     rg::MeshDevice mesh;
     std::vector<int32_t> host_car_count;
@@ -149,6 +157,89 @@ __global__ void __launch_bounds__(32) tick_kernel(TickArgs a, int ticks) {
     a.ball_world[e] = s;
 }
 
+// Car import (reference CanonicalizeImportedCarStatesInPlace, src/rocketgpu.cpp:355-379): the working fields behind
+// the report fields come back, training history resets, pos/vel go through the same uu -> bt nudge as the ball, and
+// the orientation becomes Bullet's quaternion of the (authoritative) basis.
+__global__ void canonicalize_cars_kernel(rg::CarState* cars, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rg::CarState& c = cars[i];
+    c.pad_frame_pos_valid = 0;
+    const uint8_t kept = c.tick_count_since_update != 0 ? rg::car_restore_working_fields(c) : 0;
+    rg::car_reset_training_history(c);
+    c.pos_bt = rg::V3{imported_linear_bt(c.pos.x), imported_linear_bt(c.pos.y), imported_linear_bt(c.pos.z)};
+    c.vel_bt = rg::V3{imported_linear_bt(c.vel.x), imported_linear_bt(c.vel.y), imported_linear_bt(c.vel.z)};
+    c.pos = c.pos_bt * 50.0f;
+    c.vel = c.vel_bt * 50.0f;
+    if (!c.basis_authoritative) {
+        rg::upload_basis_from_rot(c.rot, c.basis_forward, c.basis_right, c.basis_up);
+        c.basis_authoritative = 1;
+    }
+    c.rot = rg::bullet_quat_from_basis(c.basis_forward, c.basis_right, c.basis_up);
+    rg::car_re_report_fields(c, kept);
+}
+
+struct CarTickArgs {
+    TickArgs base;
+    rg::CarState* cars;
+    rg::WheelRuntime* wheels;
+    const rg::CarConfig* car_cfgs;
+    rg::PadState* pads;  // null while pads are not live
+    const rg::CarControls* controls;
+    int32_t control_stride;
+    int32_t max_cars;
+    rg::PadLayout pad_layout;
+};
+
+// Arenas with cars: ball, env and manifold scratch in registers as in tick_kernel; cars, wheel records and pads are
+// edited in place in global memory (L1-cached).
+__global__ void __launch_bounds__(32) car_tick_kernel(CarTickArgs a, int ticks) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.base.env_count) return;
+    rg::BallState b = a.base.balls[e];
+    rg::EnvState env = a.base.envs[e];
+    rg::BallWorldScratch s = a.base.ball_world[e];
+    const int car_base = e * a.max_cars;
+    rg::ArenaCars A;
+    A.cars = a.cars + car_base;
+    A.wheels = a.wheels + car_base;
+    A.cfgs = a.car_cfgs + car_base;
+    A.pads = a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr;
+    A.count = a.base.env_car_count[e];
+    A.max_cars = a.max_cars;
+    A.car_base = car_base;
+    for (int t = 0; t < ticks; ++t) {
+        A.controls = a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base;
+        rg::arena_tick_cars(env, b, s, a.base.tc, a.base.mesh, A, a.pad_layout, t + 1 == ticks);
+    }
+    a.base.balls[e] = b;
+    a.base.envs[e] = env;
+    a.base.ball_world[e] = s;
+}
+
+void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s) {
+    CarTickArgs a;
+    a.base.balls = b->balls.ptr;
+    a.base.envs = b->envs.ptr;
+    a.base.env_car_count = b->env_car_count.ptr;
+    a.base.ball_world = b->ball_world.ptr;
+    a.base.env_count = b->env_count;
+    a.base.tc = b->tc;
+    a.base.mesh = b->mesh;
+    a.cars = b->cars.ptr;
+    a.wheels = b->wheels.ptr;
+    a.car_cfgs = b->car_cfgs.ptr;
+    a.pads = b->pads_live ? b->pads.ptr : nullptr;
+    a.controls = controls;
+    a.control_stride = stride;
+    a.max_cars = b->max_cars;
+    a.pad_layout = b->pad_layout;
+    const int threads = b->launch_threads;
+    const int blocks = (b->env_count + threads - 1) / threads;
+    car_tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
+    check(cudaGetLastError(), "car_tick_kernel launch");
+}
+
 void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
     TickArgs a;
     a.balls = b->balls.ptr;
@@ -183,6 +274,13 @@ rg::TickConfig resolve_tick_config(const rg_sim_config& c) {
     t.goal_base_threshold_y = c.goal_base_threshold_y;
     t.frame_frac = 0.5f;
     t.enable_scoring = c.enable_scoring;
+    t.enable_boost_pads = c.enable_boost_pads;
+    t.max_cars = c.max_cars_per_env;
+    t.pad_count = 34;
+    t.car_mass = c.car_mass;
+    t.car_max_speed = c.car_max_speed;
+    t.car_max_ang_speed = c.car_max_ang_speed;
+    rg::fill_car_constants(t);
     return t;
 }
 
@@ -243,6 +341,56 @@ RG_API void rg_default_env_state(rg_env_state* o) {
     o->frame_frac_prev = 0.5f;
 }
 
+RG_API void rg_default_car_state(rg_car_state* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->pos = {0.0f, 0.0f, 17.0f};
+    o->rot = {1.0f, 0.0f, 0.0f, 0.0f};
+    o->boost = 100.0f;
+    o->boost_amount = 1.0f;
+    o->is_on_ground = 1;
+    for (int i = 0; i < 4; ++i) o->wheels_with_contact[i] = 1;
+    o->pos_bt = {0.0f, 0.0f, 17.0f * (1.0f / 50.0f)};
+    o->tick_start_pos_bt = o->pos_bt;
+    o->pad_frame_pos_bt = o->pos_bt;
+    o->vel_touched_solve_stage = 1;
+    o->basis_forward = {1.0f, 0.0f, 0.0f};
+    o->basis_right = {0.0f, 1.0f, 0.0f};
+    o->basis_up = {0.0f, 0.0f, 1.0f};
+    o->previous_ball_contact_start = o->last_ball_contact_start = o->last_world_surface_contact = ~0ull;
+    o->first_world_after_previous_ball = o->first_world_after_last_ball = ~0ull;
+    o->last_flip_or_jump_start = o->last_directional_flip_start = ~0ull;
+    o->flip_or_jump_last_tick = 1;
+    o->dodge_timeout = -1.0f;
+    o->latest_touch_tick = ~0ull;
+    o->double_jump_ticks = 255;
+    o->cal_pre_pitchlock_restart_time = -1.0f;
+    o->tick_start_basis_forward = {1.0f, 0.0f, 0.0f};
+    o->tick_start_basis_right = {0.0f, 1.0f, 0.0f};
+    o->tick_start_basis_up = {0.0f, 0.0f, 1.0f};
+}
+
+RG_API void rg_default_car_config(rg_car_config* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->hitbox_size = {118.00738f + 2.5f, 84.19941f + 2.5f, 36.159073f + 2.5f};
+    o->hitbox_published = {118.00738f, 84.19941f, 36.159073f};
+    o->hitbox_offset = {13.87566f, 0.0f, 20.754988f};
+    o->front_wheels_offset = {51.25f, 25.90f, 20.754988f};
+    o->back_wheels_offset = {-33.75f, 29.50f, 20.754988f};
+    o->front_wheel_radius = 12.50f;
+    o->back_wheel_radius = 15.00f;
+    o->front_suspension_rest = 38.75499f;
+    o->back_suspension_rest = 37.054989f;
+    o->dodge_deadzone = 0.5f;
+    o->three_wheels = 0;
+    o->body = 147;
+    const float steer[6] = {30.570510864257812f, 18.294261932373047f, 10.429570198059082f,
+                            6.0558881759643555f, 4.874049186706543f, 1.9791786670684814f};
+    std::memcpy(o->steer_angle_curve_deg, steer, sizeof(steer));
+    o->powerslide_steer_angle_curve_deg[0] = 22.478458404541016f;
+    o->powerslide_steer_angle_curve_deg[1] = 7.224311351776123f;
+    o->spawn_z = 36.02f;
+}
+
 RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layout, int device, rg_batch** out) {
     return guard([&] {
         if (!cfg || !layout || !out) throw std::invalid_argument("null argument");
@@ -270,6 +418,52 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         for (auto& x : balls) rg_default_ball_state(&x);
         for (auto& x : envs) rg_default_env_state(&x);
         b->host_car_count.assign(b->env_count, 0);
+        // cars, wheel records, configs, controls and pads at the reference's initial values
+        // (src/rocketgpu.cpp:1085-1130; the layout's pads are the 34 soccar pads, rocketgpu.cpp:2754-2759)
+        const size_t cap = static_cast<size_t>(b->env_count) * static_cast<size_t>(b->max_cars);
+        {
+            static const float kPads[34][3] = {
+                {0, -4240, 70},    {-1792, -4184, 70}, {1792, -4184, 70},  {-940, -3308, 70},  {940, -3308, 70},
+                {0, -2816, 70},    {-3584, -2484, 70}, {3584, -2484, 70},  {-1788, -2302, 70}, {1788, -2302, 70},
+                {-2048, -1036, 70}, {0, -1024, 70},    {2048, -1036, 70},  {-1024, 0, 70},     {1024, 0, 70},
+                {-2048, 1036, 70}, {0, 1024, 70},      {2048, 1036, 70},   {-1788, 2302, 70},  {1788, 2302, 70},
+                {-3584, 2484, 70}, {3584, 2484, 70},   {0, 2816, 70},      {-940, 3308, 70},   {940, 3308, 70},
+                {-1792, 4184, 70}, {1792, 4184, 70},   {0, 4240, 70},      {-3584, 0, 73},     {3584, 0, 73},
+                {-3072, 4096, 73}, {3072, 4096, 73},   {-3072, -4096, 73}, {3072, -4096, 73}};
+            b->pad_layout.count = 34;
+            for (int p = 0; p < 34; ++p) {
+                b->pad_layout.pos[p] = rg::V3{kPads[p][0], kPads[p][1], kPads[p][2]};
+                b->pad_layout.is_big[p] = p >= 28 ? 1 : 0;
+            }
+        }
+        b->cars.alloc(cap);
+        b->wheels.alloc(cap);
+        b->car_cfgs.alloc(cap);
+        b->controls.alloc(cap);
+        b->pads.alloc(static_cast<size_t>(b->env_count) * 34);
+        if (cap) {
+            rg_car_state c0;
+            rg_default_car_state(&c0);
+            rg_car_config k0;
+            rg_default_car_config(&k0);
+            std::vector<rg_car_state> cars(cap, c0);
+            std::vector<rg_car_config> cfgs(cap, k0);
+            std::vector<rg::WheelRuntime> wheels(cap, rg::wheel_runtime_default());
+            check(cudaMemcpy(b->cars.ptr, cars.data(), cap * sizeof(rg_car_state), cudaMemcpyHostToDevice), "cars");
+            check(cudaMemcpy(b->car_cfgs.ptr, cfgs.data(), cap * sizeof(rg_car_config), cudaMemcpyHostToDevice),
+                  "car configs");
+            check(cudaMemcpy(b->wheels.ptr, wheels.data(), cap * sizeof(rg::WheelRuntime), cudaMemcpyHostToDevice),
+                  "wheels");
+            check(cudaMemset(b->controls.ptr, 0, cap * sizeof(rg::CarControls)), "controls");
+        }
+        {
+            std::vector<rg::PadState> pads(static_cast<size_t>(b->env_count) * 34);
+            for (size_t i = 0; i < pads.size(); ++i) {
+                pads[i] = rg::PadState{0.0f, 1, static_cast<uint8_t>((i % 34) >= 28 ? 1 : 0), 32768, 0, 0};
+            }
+            check(cudaMemcpy(b->pads.ptr, pads.data(), pads.size() * sizeof(rg::PadState), cudaMemcpyHostToDevice),
+                  "pads");
+        }
         check(cudaMemcpy(b->balls.ptr, balls.data(), balls.size() * sizeof(rg_ball_state), cudaMemcpyHostToDevice),
               "upload balls");
         check(cudaMemcpy(b->envs.ptr, envs.data(), envs.size() * sizeof(rg_env_state), cudaMemcpyHostToDevice),
@@ -301,11 +495,10 @@ RG_API int rg_batch_set_env_car_count(rg_batch* b, const int32_t* counts, size_t
         for (size_t i = 0; i < count; ++i) {
             if (counts[i] < 0 || counts[i] > b->max_cars)
                 throw std::out_of_range("env car count out of range [0, max_cars_per_env]");
-            if (counts[i] != 0)
-                throw std::invalid_argument("this build steps ball-only arenas: env car counts must be 0");
         }
         DeviceGuard dg(b->device);
         std::memcpy(b->host_car_count.data(), counts, count * sizeof(int32_t));
+        for (size_t i = 0; i < count; ++i) b->pads_live = b->pads_live || counts[i] > 0;
         check(cudaMemcpyAsync(b->env_car_count.ptr, counts, count * sizeof(int32_t), cudaMemcpyHostToDevice,
                               static_cast<cudaStream_t>(stream)),
               "set_env_car_count");
@@ -373,13 +566,110 @@ RG_API int rg_batch_download_env_states(rg_batch* b, rg_env_state* host, size_t 
     });
 }
 
+}  // extern "C"
+
+namespace {
+template <class T, class D>
+void upload_array(rg_batch* b, DeviceArray<D>& dst, const T* host, size_t count, size_t cap, const char* what,
+                  void* stream) {
+    static_assert(sizeof(T) == sizeof(D), "layout");
+    if (!b || (!host && count)) throw std::invalid_argument("null argument");
+    if (count > cap) throw std::out_of_range(std::string(what) + " count exceeds capacity");
+    if (!count) return;
+    DeviceGuard dg(b->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    check(cudaMemcpyAsync(dst.ptr, host, count * sizeof(T), cudaMemcpyHostToDevice, s), what);
+    check(cudaStreamSynchronize(s), what);
+}
+template <class T, class D>
+void download_array(rg_batch* b, const DeviceArray<D>& src, T* host, size_t count, size_t cap, const char* what,
+                    void* stream) {
+    static_assert(sizeof(T) == sizeof(D), "layout");
+    if (!b || (!host && count)) throw std::invalid_argument("null argument");
+    if (count > cap) throw std::out_of_range(std::string(what) + " count exceeds capacity");
+    if (!count) return;
+    DeviceGuard dg(b->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    check(cudaMemcpyAsync(host, src.ptr, count * sizeof(T), cudaMemcpyDeviceToHost, s), what);
+    check(cudaStreamSynchronize(s), what);
+}
+}  // namespace
+
+extern "C" {
+
+RG_API int rg_batch_upload_car_states(rg_batch* b, const rg_car_state* host, size_t count, void* stream) {
+    return guard([&] {
+        upload_array(b, b->cars, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "upload_car_states",
+                     stream);
+        if (!count) return;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        canonicalize_cars_kernel<<<(static_cast<int>(count) + 127) / 128, 128, 0, s>>>(b->cars.ptr,
+                                                                                       static_cast<int>(count));
+        check(cudaGetLastError(), "canonicalize cars launch");
+        check(cudaStreamSynchronize(s), "upload_car_states sync");
+    });
+}
+RG_API int rg_batch_download_car_states(rg_batch* b, rg_car_state* host, size_t count, void* stream) {
+    return guard([&] {
+        download_array(b, b->cars, host, count, static_cast<size_t>(rg_batch_car_capacity(b)),
+                       "download_car_states", stream);
+    });
+}
+RG_API int64_t rg_batch_pad_capacity(const rg_batch* b) { return b ? static_cast<int64_t>(b->env_count) * 34 : 0; }
+RG_API int rg_batch_upload_pad_states(rg_batch* b, const rg_boost_pad_state* host, size_t count, void* stream) {
+    return guard([&] {
+        upload_array(b, b->pads, host, count, static_cast<size_t>(rg_batch_pad_capacity(b)), "upload_pad_states",
+                     stream);
+        if (count) b->pads_live = true;
+    });
+}
+RG_API int rg_batch_download_pad_states(rg_batch* b, rg_boost_pad_state* host, size_t count, void* stream) {
+    return guard([&] {
+        download_array(b, b->pads, host, count, static_cast<size_t>(rg_batch_pad_capacity(b)), "download_pad_states",
+                       stream);
+    });
+}
+RG_API int rg_batch_set_car_configs(rg_batch* b, const rg_car_config* host, size_t count, void* stream) {
+    return guard([&] {
+        for (size_t i = 0; host && i < count; ++i)
+            if (host[i].three_wheels) throw std::invalid_argument("three-wheel car configs are not supported");
+        upload_array(b, b->car_cfgs, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "set_car_configs",
+                     stream);
+    });
+}
+RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream) {
+    return guard([&] {
+        upload_array(b, b->controls, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "upload_controls",
+                     stream);
+    });
+}
+
 RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream) {
     return guard([&] {
         if (!b) throw std::invalid_argument("null argument");
         if (ticks < 0) throw std::invalid_argument("ticks must be >= 0");
         if (ticks == 0) return;
         DeviceGuard dg(b->device);
-        launch_tick(b, ticks, static_cast<cudaStream_t>(stream));
+        if (b->pads_live) {
+            launch_car_tick(b, b->controls.ptr, 0, ticks, static_cast<cudaStream_t>(stream));
+        } else {
+            launch_tick(b, ticks, static_cast<cudaStream_t>(stream));
+        }
+    });
+}
+
+RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls* device_controls, int32_t ticks,
+                                              int32_t control_stride, void* stream) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        if (ticks <= 0) return;
+        if (!device_controls) throw std::invalid_argument("device_controls_by_tick must not be null");
+        if (control_stride != 0 && static_cast<int64_t>(control_stride) < rg_batch_car_capacity(b))
+            throw std::invalid_argument("control_stride must be zero or at least the total car capacity");
+        if (control_stride < 0) throw std::invalid_argument("control_stride must be zero or at least the car capacity");
+        DeviceGuard dg(b->device);
+        launch_car_tick(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
+                        static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -422,6 +712,9 @@ RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out) {
         out->ball_states = b->balls.ptr;
         out->env_states = b->envs.ptr;
         out->env_car_count = b->env_car_count.ptr;
+        out->car_states = b->cars.ptr;
+        out->boost_pad_states = b->pads.ptr;
+        out->controls = b->controls.ptr;
     });
 }
 
@@ -467,6 +760,7 @@ RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, r
         if (env_count > kStaticScratchEnvs)
             throw std::out_of_range("env_count exceeds the static scratch capacity (4096 arenas)");
         if (ticks < 0) throw std::invalid_argument("ticks must be >= 0");
+        if (b->pads_live) throw std::invalid_argument("rg_batch_step_static_scratch steps ball-only batches");
         DeviceGuard dg(b->device);
         rg::BallWorldScratch* scratch = static_scratch_address(b->device);
         cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -63,6 +63,14 @@ RG_HD int ctz32(uint32_t x) {
 #endif
 }
 
+RG_HD int ctz64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __ffsll(static_cast<long long>(x)) - 1;
+#else
+    return __builtin_ctzll(x);
+#endif
+}
+
 RG_HD uint32_t f2u(float f) {
     uint32_t u;
     memcpy(&u, &f, 4);

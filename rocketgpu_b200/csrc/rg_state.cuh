@@ -66,6 +66,22 @@ struct TickConfig {
     float goal_base_threshold_y;
     float frame_frac;
     uint8_t enable_scoring;
+    // car-side constants (reference MutatorConfig defaults, include/rocketgpu/rocketgpu.h:708-817)
+    uint8_t enable_boost_pads;
+    int32_t max_cars;
+    int32_t pad_count;
+    float car_mass, car_max_speed, car_max_ang_speed, car_air_throttle_accel;
+    float boost_max, boost_used_per_second, boost_min_time, boost_accel_ground, boost_spawn_amount;
+    float recharge_boost_per_second, recharge_boost_delay;
+    uint8_t recharge_boost_enabled, unlimited_flips, unlimited_double_jumps;
+    float jump_accel, jump_immediate_speed, jump_min_time, jump_reset_time_pad, jump_max_time, doublejump_max_delay;
+    float flip_torque_time, flip_pitchlock_extra_time, flip_initial_vel_scale, flip_torque_x, flip_torque_y;
+    float flip_forward_impulse_max_speed_scale, flip_side_impulse_max_speed_scale,
+        flip_backward_impulse_max_speed_scale, flip_backward_impulse_scale_x;
+    float supersonic_start_speed, supersonic_maintain_min_speed, supersonic_maintain_max_time;
+    float car_air_control_pitch, car_air_control_yaw, car_air_control_roll;
+    float car_air_damp_pitch, car_air_damp_yaw, car_air_damp_roll;
+    float boost_pad_cooldown_small, boost_pad_cooldown_big, demo_respawn_time;
 };
 
 }  // namespace rg

@@ -9,6 +9,8 @@
 
 #include "rg_ball_world.cuh"
 #include "rg_math.cuh"
+#include "rg_pads.cuh"
+#include "rg_vehicle.cuh"
 #include "rg_mesh.h"
 #include "rg_state.cuh"
 
@@ -128,8 +130,8 @@ RG_HDI void ball_finish(BallState& b) {
 }
 
 // Goal test against the mouth planes and the render-frame bookkeeping (reference StepEnvTail, env_step.hpp:7006-7045;
-// CountdownUpdateTimers :6516-6537).
-RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c) {
+// CountdownUpdateTimers :6516-6537). The countdown's end re-enables driving of the arena's first `count` car slots.
+RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState* cars = nullptr, int count = 0) {
     ball_finish(b);
     if (c.enable_scoring) {
         const float score_threshold = c.goal_base_threshold_y + c.ball_radius;
@@ -161,6 +163,7 @@ RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c) {
                     if (++env.countdown_fires == 3) {
                         env.countdown_phase = 0;
                         env.countdown_fires = 0;
+                        for (int i = 0; i < count; ++i) cars[i].driving_disabled = 0;
                         b.constrained_2d = 0;
                     }
                 }
@@ -242,6 +245,138 @@ RG_HDI void arena_tick(EnvState& env, BallState& b, BallWorldScratch& s, const T
     ball_clamp_and_drag(b, c);
     ball_world_step(b, s, c, mesh);
     env_tail(env, b, c);
+}
+
+// ---- arenas with cars --------------------------------------------------------------------------------------------
+// One arena's cars during a tick: its max_cars slots of car state, wheel records and configs, its pads (null when the
+// batch never had a car, so every pad is still at its initial state) and this tick's control row.
+struct ArenaCars {
+    CarState* cars;
+    WheelRuntime* wheels;
+    const CarConfig* cfgs;
+    PadState* pads;
+    const CarControls* controls;
+    int count, max_cars, car_base;
+};
+
+// The slot visited k-th (reference CarVisitSlot, rocketgpu.h:575-581).
+RG_HD int car_visit_slot(const EnvState& env, int k, int count) {
+    if (env.car_visit_order_mode == 1 || env.car_visit_order_mode == 3)
+        return static_cast<int>((env.car_visit_order_packed >> (4 * k)) & 0xFu);
+    if (env.car_visit_order_mode == 2) return count - 1 - k;
+    return k;
+}
+// The game's vehicle order kept across demolitions (reference UpdateGameCarVisitOrder, rocketgpu.h:592-634).
+RG_HDI void update_game_visit_order(EnvState& env, const CarState* cars, int count) {
+    if (env.car_visit_order_mode != 3) return;
+    int order[8];
+    for (int k = 0; k < 8; ++k) order[k] = static_cast<int>((env.car_visit_order_packed >> (4 * k)) & 0xFu);
+    uint32_t present = env.car_visit_present_mask;
+    auto is_present = [&](int slot) { return slot < count && ((present >> slot) & 1u) != 0u; };
+    auto last_present = [&]() {
+        int q = -1;
+        for (int k = 0; k < 8; ++k)
+            if (is_present(order[k])) q = k;
+        return q;
+    };
+    for (int s = 0; s < count && s < 8; ++s) {
+        if (((present >> s) & 1u) || cars[s].is_demoed) continue;
+        int p = 0;
+        while (order[p] != s) ++p;
+        const int dst = last_present() + 1;
+        for (int k = p; k > dst; --k) order[k] = order[k - 1];
+        order[dst < p ? dst : p] = s;
+        present |= 1u << s;
+    }
+    for (int s = 0; s < count && s < 8; ++s) {
+        if (!((present >> s) & 1u) || !cars[s].is_demoed) continue;
+        int p = 0;
+        while (order[p] != s) ++p;
+        const int q = last_present();
+        order[p] = order[q];
+        order[q] = s;
+        present &= ~(1u << s);
+    }
+    uint32_t packed = 0;
+    for (int k = 0; k < 8; ++k) packed |= (static_cast<uint32_t>(order[k]) & 0xFu) << (4 * k);
+    env.car_visit_order_packed = packed;
+    env.car_visit_present_mask = static_cast<uint8_t>(present);
+}
+
+// A car's tick start (reference StepEnvPreTickCar, env_step.hpp:6751-6873): working fields back from the report
+// fields, internal clocks after a state set, the demolition timer, the tick-start quantization, the pre-physics
+// control logic and the rigid-body speed clamp.
+RG_HDI void car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w) {
+    c.ball_contact_this_tick = 0;
+    restore_step_fields(c);
+    if (c.tick_count_since_update == 0) cal_internal_timers_from_set_state(c, tc);
+    if (c.just_respawned) c.just_respawned = 0;
+    if (c.is_demoed) {
+        c.demo_respawn_timer = fmax_(0.0f, c.demo_respawn_timer - tc.tick_dt);
+        if (!(c.demo_respawn_timer <= 0.0f) && !(fmax_(0.0f, c.demo_respawn_timer - tc.tick_dt) > 0.0f) &&
+            !(c.respawn_slot_override_plus1 >= kKickoffSpawnOverridePlus1 &&
+              c.respawn_slot_override_plus1 < kKickoffSpawnOverridePlus1 + 5)) {
+            c.boost = tc.boost_spawn_amount;
+            c.boost_amount = c.boost / 100.0f;
+        }
+    }
+    c.tick_start_pos_bt = c.pos_bt;
+    car_tick_start_quantize(c, tc);
+    const Q4 snap_rot = c.rot;
+    const V3 snap_vel = c.vel;
+    cal_flip_z_damp_prepass(c, tc);
+    c.cal_tick_start_ang_vel = c.ang_vel;
+    const V3 before = c.vel_bt;
+    car_pre_physics(c, k, cfg, tc, w, snap_rot, snap_vel);
+    if (!c.is_demoed) {
+        const bool impulsed = c.vel_bt.x != before.x || c.vel_bt.y != before.y || c.vel_bt.z != before.z;
+        if ((car_body_damping_clamp(c, tc) & 1) && impulsed) car_set_vel_bt(c, c.vel_bt);
+    }
+}
+
+// One tick of one arena with cars (reference StepEnvGeneric, env_step.hpp:7088-7180, and WorldStepSoccar for cars
+// that touch nothing but the air: car contacts with the arena, the ball and each other are not built yet).
+RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, const TickConfig& c,
+                            const MeshDevice& mesh, const ArenaCars& A, const PadLayout& pads_layout,
+                            bool report_fields) {
+    const int count = A.count;
+    update_game_visit_order(env, A.cars, count);
+    env.goal_scored_this_tick = 0;
+    int order[8];
+    for (int k = 0; k < count; ++k) order[k] = car_visit_slot(env, k, count);
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        car_pre_tick(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i]);
+    }
+    ball_tick_start_quantize(b, c);
+    ball_clamp_and_drag(b, c);
+    if (c.enable_boost_pads && count > 0 && A.pads)
+        for (int p = 0; p < pads_layout.count; ++p) pad_pre_tick(A.pads[p], c.tick_dt);
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh);
+    }
+    PreContactCar pre[8];
+    for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, c.tick_dt, pre[i]);
+    ball_world_step(b, s, c, mesh);
+    for (int i = 0; i < count; ++i) car_world_finish(A.cars[i], pre[i], c.tick_dt);
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        CarState& car = A.cars[i];
+        car_post_tick(car, A.controls[i], c.tick_dt);
+        car_finish_tick(car);
+        if (report_fields) {
+            report_rlbot_fields(car, A.wheels[i], c);
+        } else {
+            advance_rlbot_fields(car, A.wheels[i], c);
+        }
+    }
+    if (A.pads) pads_tail(A.cars, A.car_base, A.max_cars, A.cfgs, count, order, A.pads, pads_layout, c);
+    for (int k = 0; k < count; ++k) {
+        CarState& car = A.cars[order[k]];
+        if (!car.is_demoed && car.driving_disabled) --car.driving_disabled;
+    }
+    env_tail(env, b, c, A.cars, count);
 }
 
 }  // namespace rg

@@ -36,3 +36,69 @@ def free_flight_states(default_ball: np.ndarray, n: int, seed: int) -> np.ndarra
 
 def ball_pos(b: np.ndarray) -> np.ndarray:
     return b[:, OFF_POS:OFF_POS + 12].copy().view(np.float32)
+
+
+# ---- cars -------------------------------------------------------------------------------------------------------------
+CAR_BYTES, CONTROLS_BYTES = 880, 24
+CAR_POS, CAR_ROT, CAR_VEL, CAR_ANG, CAR_ON_GROUND = 0, 12, 28, 40, 122
+
+
+def _yaw_quat(yaw):
+    return np.stack([np.cos(yaw / 2), np.zeros_like(yaw), np.zeros_like(yaw), np.sin(yaw / 2)], 1)
+
+
+def airborne_cars(template: np.ndarray, n: int, seed: int, z: float = 1000.0) -> np.ndarray:
+    """One car per row high above the floor: seeded position, uniform random orientation, slow linear and angular
+    velocity, not on the ground (the cars fall freely for about 100 ticks)."""
+    rng = np.random.default_rng(seed)
+    out = np.tile(np.asarray(template, np.uint8).reshape(1, CAR_BYTES), (n, 1))
+    pos = np.stack([rng.uniform(-2000, 2000, n), rng.uniform(-3000, 3000, n), np.full(n, z)], 1).astype(np.float32)
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    out[:, CAR_POS:CAR_POS + 12] = pos.view(np.uint8).reshape(n, 12)
+    out[:, CAR_ROT:CAR_ROT + 16] = q.astype(np.float32).view(np.uint8).reshape(n, 16)
+    out[:, CAR_VEL:CAR_VEL + 12] = rng.uniform(-300, 300, (n, 3)).astype(np.float32).view(np.uint8).reshape(n, 12)
+    out[:, CAR_ANG:CAR_ANG + 12] = rng.uniform(-2, 2, (n, 3)).astype(np.float32).view(np.uint8).reshape(n, 12)
+    out[:, CAR_ON_GROUND] = 0
+    return out
+
+
+def grounded_cars(template: np.ndarray, n: int, seed: int) -> np.ndarray:
+    """One car per row resting on its wheels near the middle of the floor with a seeded heading and speed."""
+    rng = np.random.default_rng(seed)
+    out = np.tile(np.asarray(template, np.uint8).reshape(1, CAR_BYTES), (n, 1))
+    pos = np.stack([rng.uniform(-1500, 1500, n), rng.uniform(-2500, 2500, n), np.full(n, 17.0)], 1).astype(np.float32)
+    yaw = rng.uniform(-np.pi, np.pi, n)
+    q = _yaw_quat(yaw)
+    speed = rng.uniform(0, 1500, n)
+    vel = np.stack([np.cos(yaw) * speed, np.sin(yaw) * speed, np.zeros(n)], 1).astype(np.float32)
+    out[:, CAR_POS:CAR_POS + 12] = pos.view(np.uint8).reshape(n, 12)
+    out[:, CAR_ROT:CAR_ROT + 16] = q.astype(np.float32).view(np.uint8).reshape(n, 16)
+    out[:, CAR_VEL:CAR_VEL + 12] = vel.view(np.uint8).reshape(n, 12)
+    return out
+
+
+class ControlStream:
+    """Seeded random controls: axes U[-1, 1], jump / boost / handbrake Bernoulli(p_jump / 0.3 / 0.1), each car's sample
+    held for U{1..hold_max} ticks."""
+
+    def __init__(self, rows: int, seed: int, p_jump: float = 0.1, hold_max: int = 1):
+        self.rng = np.random.default_rng(seed)
+        self.rows, self.p_jump, self.hold_max = rows, p_jump, hold_max
+        self.cur = np.zeros((rows, CONTROLS_BYTES), np.uint8)
+        self.left = np.zeros(rows, np.int64)
+
+    def next(self) -> np.ndarray:
+        renew = self.left <= 0
+        k = int(renew.sum())
+        if k:
+            f = self.rng.uniform(-1, 1, (k, 5)).astype(np.float32)
+            row = np.zeros((k, CONTROLS_BYTES), np.uint8)
+            row[:, :20] = f.view(np.uint8).reshape(k, 20)
+            row[:, 20] = self.rng.random(k) < self.p_jump
+            row[:, 21] = self.rng.random(k) < 0.3
+            row[:, 22] = self.rng.random(k) < 0.1
+            self.cur[renew] = row
+            self.left[renew] = self.rng.integers(1, self.hold_max + 1, k)
+        self.left -= 1
+        return self.cur.copy()

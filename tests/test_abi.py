@@ -28,6 +28,14 @@ def test_defaults_match_reference_structs(oracle_available):
     lib.rg_default_env_state(my_env.ctypes.data)
     assert bytes(my_ball) == bytes(ball)
     assert bytes(my_env) == bytes(env)
+    my_car = np.zeros(880, np.uint8)
+    my_cfg = np.zeros(120, np.uint8)
+    lib.rg_default_car_state(my_car.ctypes.data)
+    lib.rg_default_car_config(my_cfg.ctypes.data)
+    assert bytes(my_car) == bytes(car), np.nonzero(my_car != car)[0]
+    pad_byte = 81  # CarConfig's padding between three_wheels (u8 at 80) and body (u16 at 82)
+    keep = np.arange(120) != pad_byte
+    assert (my_cfg[keep] == cfg[keep]).all(), np.nonzero(my_cfg != cfg)[0]
 
 
 def test_ucrt_math_matches_reference(oracle_available):
