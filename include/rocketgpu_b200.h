@@ -240,6 +240,14 @@ RG_API int rg_batch_download_pad_states(rg_batch* b, rg_boost_pad_state* host, s
 /* BatchSim::set_car_configs (rocketgpu.h:1025). Three-wheel configs are rejected (invalid_argument): that car
  * model is not built. */
 RG_API int rg_batch_set_car_configs(rg_batch* b, const rg_car_config* host, size_t count, void* stream);
+/* BatchSim::set_teams (rocketgpu.h:1024): team per car slot, 0 blue / 1 orange (the reference's Team enum). */
+RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, void* stream);
+/* BatchSim::reset_to_kickoff (rocketgpu.h:1070; src/rocketgpu.cpp:2085-2132, ResetEnvToKickoff arena_ball.hpp:
+ * 3054-3085): every arena to kickoff, the spot order drawn from `seed` (0: from the arena's reset count). Car
+ * contact state and the ball's manifolds are cleared; wheel records are kept, as the reference keeps them.
+ * rg_batch_create ends with reset_to_kickoff(0). Kickoff-settle copies (SimConfig.kickoff_settled) are not built:
+ * the reset is the reference's with kickoff_settled = 0. */
+RG_API int rg_batch_reset_to_kickoff(rg_batch* b, uint64_t seed, void* stream);
 /* BatchSim::upload_controls (rocketgpu.h:1032): the controls rg_batch_step holds for every tick. */
 RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream);
 

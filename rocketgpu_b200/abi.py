@@ -21,7 +21,8 @@ EXPORTS = [
     "rg_arena_mesh_tables", "rg_batch_step_static_scratch",
     "rg_default_car_state", "rg_default_car_config", "rg_batch_upload_car_states", "rg_batch_download_car_states",
     "rg_batch_pad_capacity", "rg_batch_upload_pad_states", "rg_batch_download_pad_states", "rg_batch_set_car_configs",
-    "rg_batch_upload_controls", "rg_batch_step_with_device_controls",
+    "rg_batch_upload_controls", "rg_batch_step_with_device_controls", "rg_batch_set_teams",
+    "rg_batch_reset_to_kickoff",
 ]
 
 
@@ -77,7 +78,7 @@ def lib():
         for n in ("rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
                   "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_upload_car_states",
                   "rg_batch_download_car_states", "rg_batch_upload_pad_states", "rg_batch_download_pad_states",
-                  "rg_batch_set_car_configs", "rg_batch_upload_controls"):
+                  "rg_batch_set_car_configs", "rg_batch_upload_controls", "rg_batch_set_teams"):
             getattr(L, n).argtypes = [vp, vp, sz, vp]
         L.rg_batch_step.argtypes = [vp, i32, vp]
         L.rg_batch_synchronize.argtypes = [vp, vp]
@@ -96,5 +97,6 @@ def lib():
         L.rg_batch_pad_capacity.argtypes = [vp]
         L.rg_batch_pad_capacity.restype = i64
         L.rg_batch_step_with_device_controls.argtypes = [vp, vp, i32, i32, vp]
+        L.rg_batch_reset_to_kickoff.argtypes = [vp, ctypes.c_uint64, vp]
         _lib = L
     return _lib

@@ -135,6 +135,13 @@ class BatchSim:
         s = np.ascontiguousarray(configs, np.uint8).reshape(-1, CAR_CONFIG_BYTES)
         _check(abi.lib().rg_batch_set_car_configs(self._h, _ptr(s), len(s), stream))
 
+    def set_teams(self, teams, stream: int = 0):
+        t = np.ascontiguousarray(teams, np.uint8)
+        _check(abi.lib().rg_batch_set_teams(self._h, _ptr(t), len(t), stream))
+
+    def reset_to_kickoff(self, seed: int = 0, stream: int = 0):
+        _check(abi.lib().rg_batch_reset_to_kickoff(self._h, seed, stream))
+
     def upload_controls(self, controls: np.ndarray, stream: int = 0):
         s = np.ascontiguousarray(controls, np.uint8).reshape(-1, CONTROLS_BYTES)
         _check(abi.lib().rg_batch_upload_controls(self._h, _ptr(s), len(s), stream))

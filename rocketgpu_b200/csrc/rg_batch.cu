@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "rg_mesh.h"
+#include "rg_reset.cuh"
 #include "rg_tick.cuh"
 #include "rg_ucrt.cuh"
 #include "rocketgpu_b200.h"
@@ -84,6 +85,7 @@ struct rg_batch {
     DeviceArray<rg::CarConfig> car_cfgs;
     DeviceArray<rg::CarControls> controls;
     DeviceArray<rg::PadState> pads;
+    DeviceArray<uint8_t> teams;
     rg::PadLayout pad_layout{};
     // Pads stay at their initial state until a car exists or pads are uploaded; until then ball-only arenas skip them.
     bool pads_live = false;
@@ -238,6 +240,38 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     const int blocks = (b->env_count + threads - 1) / threads;
     car_tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
     check(cudaGetLastError(), "car_tick_kernel launch");
+}
+
+// reset_to_kickoff for every arena (reference BatchSim::reset_to_kickoff, src/rocketgpu.cpp:2085-2132).
+__global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::CarControls* controls, uint64_t seed) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.base.env_count) return;
+    const int car_base = e * a.max_cars;
+    rg::reset_env_to_kickoff(e, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
+                             a.car_cfgs + car_base, controls + car_base,
+                             a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
+                             teams + car_base, a.base.env_car_count[e], a.max_cars, a.base.tc);
+}
+
+void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
+    CarTickArgs a;
+    a.base.balls = b->balls.ptr;
+    a.base.envs = b->envs.ptr;
+    a.base.env_car_count = b->env_car_count.ptr;
+    a.base.ball_world = b->ball_world.ptr;
+    a.base.env_count = b->env_count;
+    a.base.tc = b->tc;
+    a.base.mesh = b->mesh;
+    a.cars = b->cars.ptr;
+    a.wheels = b->wheels.ptr;
+    a.car_cfgs = b->car_cfgs.ptr;
+    a.pads = b->pads.ptr;
+    a.controls = nullptr;
+    a.control_stride = 0;
+    a.max_cars = b->max_cars;
+    a.pad_layout = b->pad_layout;
+    reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed);
+    check(cudaGetLastError(), "reset_kickoff_kernel launch");
 }
 
 void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
@@ -441,6 +475,8 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         b->car_cfgs.alloc(cap);
         b->controls.alloc(cap);
         b->pads.alloc(static_cast<size_t>(b->env_count) * 34);
+        b->teams.alloc(cap);
+        if (cap) check(cudaMemset(b->teams.ptr, 0, cap), "teams");
         if (cap) {
             rg_car_state c0;
             rg_default_car_state(&c0);
@@ -471,6 +507,9 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         check(cudaMemcpy(b->env_car_count.ptr, b->host_car_count.data(), b->env_count * sizeof(int32_t),
                          cudaMemcpyHostToDevice),
               "upload car counts");
+        // BatchSim's constructor ends with reset_to_kickoff(0) (src/rocketgpu.cpp:1281)
+        launch_reset(b.get(), 0, nullptr);
+        check(cudaDeviceSynchronize(), "initial kickoff reset");
         *out = b.release();
     });
 }
@@ -635,6 +674,20 @@ RG_API int rg_batch_set_car_configs(rg_batch* b, const rg_car_config* host, size
             if (host[i].three_wheels) throw std::invalid_argument("three-wheel car configs are not supported");
         upload_array(b, b->car_cfgs, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "set_car_configs",
                      stream);
+    });
+}
+RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, void* stream) {
+    return guard([&] {
+        for (size_t i = 0; host && i < count; ++i)
+            if (host[i] > 1) throw std::invalid_argument("team must be 0 (blue) or 1 (orange)");
+        upload_array(b, b->teams, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "set_teams", stream);
+    });
+}
+RG_API int rg_batch_reset_to_kickoff(rg_batch* b, uint64_t seed, void* stream) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        DeviceGuard dg(b->device);
+        launch_reset(b, seed, static_cast<cudaStream_t>(stream));
     });
 }
 RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream) {

@@ -1,0 +1,263 @@
+// Kickoff reset of one arena: the env's kickoff bookkeeping (the match's shuffled kickoff spots and respawn order),
+// the ball at its kickoff rest, every pad active, controls cleared, and each car at its team's kickoff spot
+// (reference ResetEnvToKickoff, include/rocketgpu/detail/step/arena_ball.hpp:2827-3085, as BatchSim::reset_to_kickoff
+// runs it: kickoff seed mode 0, no platform respawn RNG, no settled-kickoff copy, score not preserved).
+#pragma once
+
+#include "rg_car.cuh"
+#include "rg_pads.cuh"
+
+namespace rg {
+
+constexpr float kHalfPiF = 1.57079632679489661923f;
+constexpr float kSqrtHalfF = 0.7071067811865475244f;
+
+struct SpawnPos {
+    float x, y, yaw;
+};
+// reference SoccarKickoffSpawn (constants.hpp:38-46)
+RG_HDI SpawnPos soccar_kickoff_spawn(int i) {
+    switch (i) {
+        case 0: return {-2048.0f, -2560.0f, kPiF * 0.25f};
+        case 1: return {2048.0f, -2560.0f, kPiF * 0.75f};
+        case 2: return {-256.0f, -3840.0f, kPiF * 0.50f};
+        case 3: return {256.0f, -3840.0f, kPiF * 0.50f};
+        default: return {0.0f, -4608.0f, kPiF * 0.50f};
+    }
+}
+
+RG_HDI uint32_t rng_advance(uint32_t s) { return s * 1664525u + 1013904223u; }
+RG_HDI uint32_t mix_seed(uint64_t seed, int env_idx, int extra) {
+    uint64_t x = seed;
+    x ^= static_cast<uint64_t>(env_idx + 0x9e3779b9U) + (x << 6U) + (x >> 2U);
+    x ^= static_cast<uint64_t>(extra + 0x85ebca6bU) + (x << 13U) + (x >> 7U);
+    return static_cast<uint32_t>(x & 0xffffffffu);
+}
+// reference BuildKickoffOrder / BuildRespawnOrder (arena_ball.hpp:2606-2640)
+RG_HDI void build_kickoff_order(uint64_t seed, int env_idx, int* order) {
+    int left[5] = {0, 1, 2, 3, 4};
+    uint32_t state = mix_seed(seed, env_idx, 0x6b1d4f2a);
+    for (int n = 5; n > 0; --n) {
+        state = rng_advance(state);
+        const int idx =
+            static_cast<int>(static_cast<float>((state >> 16) & 0x7fffu) * (1.0f / 32768.0f) * static_cast<float>(n));
+        order[5 - n] = left[idx];
+        for (int i = idx; i + 1 < n; ++i) left[i] = left[i + 1];
+    }
+}
+RG_HDI uint8_t build_respawn_order(uint64_t seed, int env_idx) {
+    uint32_t left = 0x3210u;
+    uint32_t state = mix_seed(seed, env_idx, 0x3c6ef372);
+    uint32_t packed = 0;
+    for (int n = 4; n > 0; --n) {
+        state = rng_advance(state);
+        const int idx =
+            static_cast<int>(static_cast<float>((state >> 16) & 0x7fffu) * (1.0f / 32768.0f) * static_cast<float>(n));
+        packed |= ((left >> (4 * idx)) & 0xFu) << (2 * (4 - n));
+        left = (left & ((1u << (4 * idx)) - 1u)) | ((left >> (4 * (idx + 1))) << (4 * idx));
+    }
+    return static_cast<uint8_t>(packed);
+}
+
+RG_HDI float wrap_angle(float a) {
+    while (a > kPiF) a -= 2.0f * kPiF;
+    while (a < -kPiF) a += 2.0f * kPiF;
+    return a;
+}
+// reference FromYaw (math.hpp:838-863)
+RG_HDI Q4 quat_from_yaw(float yaw) {
+    constexpr float kEps = 1e-6f;
+    constexpr float kSin8 = 0.38268343236508977173f;
+    constexpr float kCos8 = 0.92387953251128675613f;
+    if (fabs_(yaw - (kPiF * 0.25f)) <= kEps) return Q4{kCos8, 0.0f, 0.0f, kSin8};
+    if (fabs_(yaw + (kPiF * 0.25f)) <= kEps) return Q4{kCos8, 0.0f, 0.0f, -kSin8};
+    if (fabs_(yaw - (kPiF * 0.75f)) <= kEps) return Q4{kSin8, 0.0f, 0.0f, kCos8};
+    if (fabs_(yaw + (kPiF * 0.75f)) <= kEps) return Q4{kSin8, 0.0f, 0.0f, -kCos8};
+    if (fabs_(yaw - kHalfPiF) <= kEps) return Q4{kSqrtHalfF, 0.0f, 0.0f, kSqrtHalfF};
+    if (fabs_(yaw + kHalfPiF) <= kEps) return Q4{kSqrtHalfF, 0.0f, 0.0f, -kSqrtHalfF};
+    const float h = 0.5f * yaw;
+    return Q4{game_cosf(h), 0.0f, 0.0f, game_sinf(h)};
+}
+RG_HDI int spawn_yaw_rotator_units(float yaw) { return static_cast<int>(yaw * (32768.0f / 3.14159274f) + 0.5f); }
+// reference SeedCarBasisFromSpawnRotator (math.hpp:1478-1490)
+RG_HDI void seed_car_basis_from_spawn(CarState& c, int blue_yaw, bool orange) {
+    Q4 q = ue3_quat_from_yaw(blue_yaw);
+    if (orange) {
+        const Q4 h = ue3_quat_from_yaw(32768);
+        q = Q4{((h.w * q.w - h.x * q.x) - h.y * q.y) - h.z * q.z, ((h.w * q.x + h.x * q.w) + h.y * q.z) - h.z * q.y,
+               ((h.w * q.y + h.y * q.w) + h.z * q.x) - h.x * q.z, ((h.w * q.z + h.z * q.w) + h.x * q.y) - h.y * q.x};
+    }
+    game_basis_from_rot(q, c.basis_forward, c.basis_right, c.basis_up);
+    c.basis_authoritative = 1;
+}
+// reference ResetCarCommonState (arena_ball.hpp:2478-2538)
+RG_HDI void reset_car_common(CarState& c, float spawn_boost) {
+    c.restored_inv_inertia_valid = 0;
+    car_set_vel_bt(c, V3{0.0f, 0.0f, 0.0f});
+    c.ang_vel = V3{0.0f, 0.0f, 0.0f};
+    memset(&c.world_contact, 0, sizeof(c.world_contact));
+    c.flip_rel_torque = V3{0.0f, 0.0f, 0.0f};
+    c.boost = spawn_boost;
+    c.boost_amount = spawn_boost / 100.0f;
+    c.jump_time = c.flip_time = c.internal_jump_time = c.internal_flip_time = 0.0f;
+    c.flip_timer_live = 1;
+    c.air_time = c.air_time_since_jump = c.boosting_time = c.time_since_boosted = 0.0f;
+    c.supersonic_time = c.handbrake_val = c.auto_flip_timer = c.auto_flip_torque_scale = 0.0f;
+    c.demo_respawn_timer = 0.0f;
+    c.tick_count_since_update = 0;
+    c.is_on_ground = 1;
+    c.air_state = 0;
+    c.rlbotv5_dodged = 0;
+    c.rlbotv5_boost_hold = 0;
+    c.dodge_timeout = -1.0f;
+    c.dodge_elapsed = c.dodge_dir_x = c.dodge_dir_y = 0.0f;
+    for (int i = 0; i < 4; ++i) c.wheels_with_contact[i] = 0;
+    c.has_jumped = c.has_double_jumped = c.has_flipped = c.is_flipping = c.is_jumping = 0;
+    c.jump_hold_broken = c.is_boosting = c.is_supersonic = c.is_auto_flipping = c.is_demoed = c.just_respawned = 0;
+    c.car_contact.other_car_id = 0;
+    c.car_contact.cooldown_timer = 0.0f;
+    c.vel_impulse_cache = c.vel_impulse_cache_bt = V3{0.0f, 0.0f, 0.0f};
+    c.pending_bump_count = 0;
+    memset(&c.ball_hit_info, 0, sizeof(c.ball_hit_info));
+    memset(&c.last_controls, 0, sizeof(c.last_controls));
+    c.boost_pad_touching = 0;
+    c.driving_disabled = 0;
+    c.respawn_slot_override_plus1 = 0;
+    c.pad_frame_pos_valid = 0;
+}
+// reference PlaceCarAtKickoffSpawn (arena_ball.hpp:2540-2560); team 0 blue, 1 orange
+RG_HDI void place_car_at_kickoff_spawn(CarState& c, int team, SpawnPos spawn, float z, float boost) {
+    float x = spawn.x, y = spawn.y, yaw = spawn.yaw;
+    if (team == 1) {
+        x = -x;
+        y = -y;
+        yaw += kPiF;
+    }
+    car_set_pos_bt(c, V3{x, y, z} * kUuToBt);
+    c.rot = quat_from_yaw(wrap_angle(yaw));
+    seed_car_basis_from_spawn(c, spawn_yaw_rotator_units(spawn.yaw), team == 1);
+    reset_car_common(c, boost);
+}
+
+// reference ResetBall(ball, Soccar, game_spawn = false) (arena_ball.hpp:2775-2815)
+RG_HDI void reset_kickoff_ball(BallState& b) {
+    b.pos_bt = V3{0.0f, 0.0f, 93.15f} * kUuToBt;
+    b.pos = b.pos_bt * 50.0f;
+    b.rot = Q4{1.0f, 0.0f, 0.0f, 0.0f};
+    b.basis_forward = V3{1.0f, 0.0f, 0.0f};
+    b.basis_right = V3{0.0f, 1.0f, 0.0f};
+    b.basis_up = V3{0.0f, 0.0f, 1.0f};
+    b.basis_authoritative = 1;
+    b.vel_bt = V3{0.0f, 0.0f, 0.0f};
+    b.vel = b.vel_bt * 50.0f;
+    b.ang_vel = V3{0.0f, 0.0f, 0.0f};
+    b.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
+    b.vel_impulse_cache_bt = V3{0.0f, 0.0f, 0.0f};
+    b.tick_count_when_extra_impulse_applied = 0;
+    b.tick_count_since_update = 0;
+    b.hs_y_target_dir = 0.0f;
+    b.hs_cur_target_speed = 2900.0f;
+    b.hs_time_since_hit = 0.0f;
+    b.ds_charge_level = 1;
+    b.ds_accumulated_hit_force = 0.0f;
+    b.ds_y_target_dir = 0.0f;
+    for (int i = 0; i < 4; ++i) b.ds_flags[i] = 0;
+    b.ds_last_damage_tick = 0;
+    b.sleeping = 0;
+    b.deactivation_time = 0.0f;
+    b.constrained_2d = 0;
+    b.pos_bt = V3{0.0f, 0.0f, 92.75f} * kUuToBt;
+    b.pos = b.pos_bt * 50.0f;
+    b.sleeping = 1;
+}
+
+// The whole arena. `teams` are the arena's max_cars slot teams (0 blue, 1 orange); `scratch` is its persistent
+// contact state, cleared as the reference clears its solver scratch.
+RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, BallState& ball, BallWorldScratch& scratch,
+                                 CarState* cars, const CarConfig* cfgs, CarControls* controls, PadState* pads,
+                                 const PadLayout& L, const uint8_t* teams, int count, int max_cars,
+                                 const TickConfig& tc) {
+    memset(&scratch, 0, sizeof(scratch));
+    const EnvState saved = env;
+    EnvState next;
+    memset(&next, 0, sizeof(next));
+    next.last_scored_team = -1;
+    next.car_visit_order_mode = 3;
+    next.car_visit_present_mask = 0xFF;
+    next.car_visit_order_packed = 0x76543210u;
+    next.frame_frac_prev = 0.5f;
+    next.kickoff_resets = static_cast<uint8_t>(saved.kickoff_resets + 1);
+    next.kickoff_match_order = saved.kickoff_match_order;
+    next.kickoff_match_index = saved.kickoff_match_index;
+    next.respawn_match_order = saved.respawn_match_order;
+    if (seed == 0) seed = saved.kickoff_resets * 0x9e3779b97f4a7c15ull;
+    next.car_visit_order_mode = saved.car_visit_order_mode;
+    next.car_visit_order_packed = saved.car_visit_order_packed;
+    if (saved.car_visit_order_mode == 3) {
+        next.car_visit_order_packed = 0x76543210u;
+        next.car_visit_present_mask = 0xFFu;
+    }
+    next.frame_ticks = saved.frame_ticks;
+    next.frame_frac_prev = saved.frame_frac_prev;
+    int kickoff_order[5];
+    build_kickoff_order(seed, env_idx, kickoff_order);
+    {
+        uint32_t packed = 0x8000u;
+        for (int j = 0; j < 5; ++j) packed |= static_cast<uint32_t>(kickoff_order[j]) << (3 * j);
+        next.kickoff_match_order = static_cast<uint16_t>(packed);
+        next.kickoff_match_index = 1;
+        next.respawn_match_order = build_respawn_order(seed, env_idx);
+    }
+    env = next;
+    uint32_t order_bits = 0;
+    for (int i = 0; i < 5; ++i) order_bits |= static_cast<uint32_t>(kickoff_order[i]) << (3 * i);
+
+    reset_kickoff_ball(ball);
+    if (pads) {
+        for (int p = 0; p < L.count; ++p) {
+            PadState& pad = pads[p];
+            pad.cooldown = 0.0f;
+            pad.is_active = 1;
+            pad.is_big = L.is_big[p];
+            pad.prev_locked_car_id = 0;
+            pad.cur_locked_car_id = 0;
+            pad.pickup_frac_q = 32768;
+        }
+    }
+    for (int i = 0; i < max_cars; ++i) memset(&controls[i], 0, sizeof(CarControls));
+    for (int i = 0; i < count; ++i) {
+        // the car's place among its team's cars in visit order picks its kickoff spot (FindKickoffCarSpot)
+        const int team = teams[i];
+        int nth = 0;
+        bool found = false;
+        for (int k = 0; k < count && !found; ++k) {
+            int s;
+            if (env.car_visit_order_mode == 1 || env.car_visit_order_mode == 3) {
+                s = static_cast<int>((env.car_visit_order_packed >> (4 * k)) & 0xFu);
+            } else {
+                s = env.car_visit_order_mode == 2 ? count - 1 - k : k;
+            }
+            if (s == i) {
+                found = true;
+            } else if (teams[s] == team) {
+                ++nth;
+            }
+        }
+        if (!found) continue;
+        const int spot = nth < 5 ? static_cast<int>((order_bits >> (3 * nth)) & 7u) : nth;
+        SpawnPos spawn;
+        if (nth >= 5) {
+            // a sixth car of a team takes a respawn spot, 250 uu further back per round of four
+            // (reference PlaceKickoffCar, arena_ball.hpp:2998-3015; SoccarRespawnSpawn, constants.hpp:48-55)
+            const int r = (nth - 5) % 4;
+            const float step = 250.0f * static_cast<float>((nth - 5) / 4);
+            const float xs[4] = {-2304.0f, -2688.0f, 2304.0f, 2688.0f};
+            spawn = SpawnPos{xs[r], -4608.0f + step, kHalfPiF};
+        } else {
+            spawn = soccar_kickoff_spawn(spot);
+        }
+        place_car_at_kickoff_spawn(cars[i], team, spawn, cfgs[i].spawn_z, tc.boost_spawn_amount);
+    }
+}
+
+}  // namespace rg

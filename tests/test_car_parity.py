@@ -98,3 +98,30 @@ def test_grounded_cars_multi_tick_launches(oracle_available, arena_mesh, seed):
         d = _compare(orc, gpu, n, excluded)
         assert d is None, f"launch {launch}: {d}"
     assert excluded.mean() <= 0.10, excluded.mean()
+
+
+def test_kickoff_reset_matches(oracle_available, arena_mesh):
+    """reset_to_kickoff with seeded team layouts: every car at its team's kickoff spot, ball, pads and env bookkeeping."""
+    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
+    v, i = arena_mesh
+    n, mc = 64, 6
+    orc = oracle_ref.OracleSim(n, mc, v, i, kickoff_settled=False)
+    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=mc, kickoff_settled=0), v, i)
+    for what, a, b in (("ball", orc.balls(), gpu.download_ball_states()), ("env", orc.envs(), gpu.download_env_states()),
+                       ("pads", orc.pads(), gpu.download_boost_pad_states())):
+        assert (a == b).all(), f"after create: {what}"
+    rng = np.random.default_rng(7)
+    counts = rng.integers(1, mc + 1, n).astype(np.int32)
+    teams = rng.integers(0, 2, n * mc).astype(np.uint8)
+    for sim in (orc, gpu):
+        sim.set_env_car_count(counts)
+        sim.set_teams(teams)
+    active = np.concatenate([np.arange(e * mc, e * mc + counts[e]) for e in range(n)])
+    for seed in (0, 0, 987654321):
+        orc.reset_to_kickoff(seed)
+        gpu.reset_to_kickoff(seed)
+        gpu.synchronize()
+        assert (orc.cars()[active] == gpu.download_car_states()[active]).all(), seed
+        assert (orc.balls() == gpu.download_ball_states()).all(), seed
+        assert (orc.envs() == gpu.download_env_states()).all(), seed
+        assert (orc.pads() == gpu.download_boost_pad_states()).all(), seed
