@@ -189,10 +189,11 @@ RG_HDI bool clamp_edge_normal(V3 edge, V3 tri_normal, V3 contact_normal, float c
 }
 
 // Internal-edge correction of a triangle contact (Bullet btAdjustInternalEdgeContacts, reference
-// MaybeAdjustArenaTriangleInternalEdgeContactT, raycast_wheels_and_contact_prep.hpp:5044-5170, with the rules a custom
-// mesh gets: edge parameters searched over [0, 1], no exact on-edge detection). Returns whether the contact was near
-// an internal edge.
+// MaybeAdjustArenaTriangleInternalEdgeContactT, raycast_wheels_and_contact_prep.hpp:5044-5170, with the game's edge
+// rules: a soccar layout installs its local triangle copy, cal_arena_local_tris, src/rocketgpu.cpp:1152-1156, and that
+// selects them for custom meshes too). Returns whether the contact was near an internal edge.
 RG_HDI bool adjust_internal_edge(const DevTri& t, V3 point_on_a, float distance, V3& io_point_b, V3& io_normal) {
+    constexpr float t_lo = 1.0e-5f, t_hi = 1.0f - 1.0e-5f;
     constexpr float kEdgeDistanceThreshold = 0.1f;
     constexpr float kMaxEdgeAngle = 2.0f * kPiF;
     const V3 tri_normal = t.normal;
@@ -204,10 +205,12 @@ RG_HDI bool adjust_internal_edge(const DevTri& t, V3 point_on_a, float distance,
     const V3 ee[3] = {t.b, t.c, t.a};
     int best = -1;
     float best_d = 1.0e30f;
+    uint32_t on_edge = 0u;
     for (int e = 0; e < 3; ++e) {
         if (fabs_(t.edge_angle[e]) >= kMaxEdgeAngle) continue;
-        const V3 nearest = closest_on_segment(contact, es[e], ee[e], 0.0f, 1.0f);
+        const V3 nearest = closest_on_segment(contact, es[e], ee[e], t_lo, t_hi);
         const float d = len(contact - nearest);
+        if (d < 1.1920928955078125e-07f) on_edge |= 1u << e;
         if (d < best_d) {
             best_d = d;
             best = e;
@@ -219,7 +222,7 @@ RG_HDI bool adjust_internal_edge(const DevTri& t, V3 point_on_a, float distance,
     const uint32_t convex_flag[3] = {kEdgeV0V1Convex, kEdgeV1V2Convex, kEdgeV2V0Convex};
     const uint32_t swap_flag[3] = {kEdgeV0V1Swap, kEdgeV1V2Swap, kEdgeV2V0Swap};
     for (int e = 0; e < 3; ++e) {
-        if (best != e) continue;
+        if (best != e && (on_edge & (1u << e)) == 0u) continue;
         const float ang = t.edge_angle[e];
         if (fabs_(ang) >= kMaxEdgeAngle) continue;
         const V3 nearest = closest_on_segment(contact, es[e], ee[e], 0.0f, 1.0f);
