@@ -679,14 +679,12 @@ RG_HDI bool mesh_ray_closest(const MeshDevice& m, V3 from, V3 to, float& out_fra
     return hit;
 }
 
-// Predictive (continuous) contact of the ball: a ray from just behind the ball's centre to where this tick's velocity
-// takes it; a hit makes a contact at the hit plane (reference PredictiveContactRayForBody body 0,
-// env_step.hpp:3894-4128). Returns the plane normal and the signed distance of the motion's end past it.
-RG_HDI bool ball_predictive_hit(const BallState& b, const MeshDevice& m, float dt, V3& out_n, float& out_dist) {
+// The ray of a body's motion this tick, from `cur` (backed off 0.04 bt) to `to`, against the mesh; a hit gives the hit
+// plane's normal (facing the ray's start) and the motion's signed distance past it (reference
+// PredictiveContactRayForBody tail, env_step.hpp:4075-4127).
+RG_HDI bool predictive_ray(const MeshDevice& m, V3 cur, V3 to, V3& out_n, float& out_dist) {
     constexpr float kCcdMotionThresholdBt = 0.02f;
     constexpr float kRayBackoffBt = 0.04f;
-    const V3 cur = b.pos_bt;
-    const V3 to = b.pos_bt + b.vel_bt * dt;
     const V3 mv{to.x - cur.x, to.y - cur.y, to.z - cur.z};
     const float m2 = mv.x * mv.x + mv.y * mv.y + mv.z * mv.z;
     if (!(m2 > kCcdMotionThresholdBt * kCcdMotionThresholdBt)) return false;
@@ -711,6 +709,11 @@ RG_HDI bool ball_predictive_hit(const BallState& b, const MeshDevice& m, float d
     out_n = n;
     out_dist = ((delta.y - ds.y) * n.y + (delta.x - ds.x) * n.x) + (delta.z - ds.z) * n.z;
     return true;
+}
+// Predictive (continuous) contact of the ball: its centre's motion this tick (reference PredictiveContactRayForBody
+// body 0, env_step.hpp:3894-4128).
+RG_HDI bool ball_predictive_hit(const BallState& b, const MeshDevice& m, float dt, V3& out_n, float& out_dist) {
+    return predictive_ray(m, b.pos_bt, b.pos_bt + b.vel_bt * dt, out_n, out_dist);
 }
 
 // --- the ball's arena contact stage ---------------------------------------------------------------------------------

@@ -94,6 +94,8 @@ inline void fill_car_constants(TickConfig& t) {
     t.boost_pad_cooldown_small = 4.0f;
     t.boost_pad_cooldown_big = 10.0f;
     t.demo_respawn_time = 3.0f;
+    t.arena_friction = 0.30f;
+    t.arena_restitution = 0.30f;
 }
 
 // ---- setters (reference arena_geometry.hpp:1799-1821) ------------------------------------------------------------

@@ -82,6 +82,7 @@ struct TickConfig {
     float car_air_control_pitch, car_air_control_yaw, car_air_control_roll;
     float car_air_damp_pitch, car_air_damp_yaw, car_air_damp_roll;
     float boost_pad_cooldown_small, boost_pad_cooldown_big, demo_respawn_time;
+    float arena_friction, arena_restitution;
 };
 
 }  // namespace rg

@@ -8,6 +8,8 @@
 #pragma once
 
 #include "rg_ball_world.cuh"
+#include "rg_broadphase.cuh"
+#include "rg_car_world.cuh"
 #include "rg_math.cuh"
 #include "rg_pads.cuh"
 #include "rg_vehicle.cuh"
@@ -334,22 +336,486 @@ RG_HDI void car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg
     }
 }
 
-// One tick of one arena with cars (reference StepEnvGeneric, env_step.hpp:7088-7180, and WorldStepSoccar for cars
-// that touch nothing but the air: car contacts with the arena, the ball and each other are not built yet).
-RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, const TickConfig& c,
-                            const MeshDevice& mesh, const ArenaCars& A, const PadLayout& pads_layout,
-                            bool report_fields) {
+// ---- the world step of an arena with cars ------------------------------------------------------------------------
+// Per-tick snapshots the world step needs from the tick start: the velocities the broadphase predicts motion with
+// (reference car_predict_vel_bt / ball_predict_vel_bt, env_step.hpp:6847-6851, 6884).
+struct TickSnap {
+    V3 ball_vel_bt;
+    V3 car_vel_bt[8], car_ang_vel[8];
+};
+
+// The car's predictive (CCD) contact: its box centre's motion this tick (reference PredictiveContactRayForBody
+// body > 0, env_step.hpp:3930-4060; the free-box shortcuts there only skip rays that cannot hit).
+RG_HDI bool car_predictive_hit(const CarState& c, const CarConfig& cfg, const MeshDevice& m, float dt, V3& n,
+                               float& dist) {
+    V3 ax, ay, az;
+    car_basis(c, ax, ay, az);
+    const V3 child = cfg.hitbox_offset * (1.0f / 50.0f);
+    const V3 cur{c.pos_bt.x + (ax.x * child.x + ay.x * child.y + az.x * child.z),
+                 c.pos_bt.y + (ax.y * child.x + ay.y * child.y + az.y * child.z),
+                 c.pos_bt.z + (ax.z * child.x + ay.z * child.y + az.z * child.z)};
+    V3 f = c.basis_forward, r = c.basis_right, u = c.basis_up;
+    Q4 rot = c.rot;
+    game_integrate_orientation(f, r, u, rot, c.ang_vel, dt);
+    const V3 po = c.pos_bt + c.vel_bt * dt;
+    const V3 to{po.x + (f.x * child.x + r.x * child.y + u.x * child.z),
+                po.y + (f.y * child.x + r.y * child.y + u.y * child.z),
+                po.z + (f.z * child.x + r.z * child.y + u.z * child.z)};
+    return predictive_ray(m, cur, to, n, dist);
+}
+
+// PGS at the velocity level over every contact row of the arena, in the order the sorted manifold list gives
+// (reference SolveUnifiedVelocityContactRowsGeneral, arena_geometry.hpp:5527-5866): for each listed manifold its rows,
+// then the unlisted car rows, then the unlisted ball rows; each normal row's friction row follows the normal order.
+// Rows act on their own body's velocity deltas; one iteration count (stop when nothing changed) covers all.
+RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const BpEntry* list, int n_list,
+                                   V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
+    constexpr int kMax = kMaxBallVelRows + kMaxCarWorldRows;
+    uint8_t nb[kMax], ni[kMax], fb[kMax], fi[kMax];
+    int nn = 0, nf = 0;
+    const int wn = cr.nv, bn = br.vel_count, wf = cr.nf, bf = br.fric_count;
+    if (wn + bn <= 1 && wf + bf <= 1) {
+        if (wn == 1) {
+            nb[0] = 0;
+            ni[0] = 0;
+            nn = 1;
+        } else if (bn == 1) {
+            nb[0] = 2;
+            ni[0] = 0;
+            nn = 1;
+        }
+        if (wf == 1) {
+            fb[0] = 0;
+            fi[0] = 0;
+            nf = 1;
+        } else if (bf == 1) {
+            fb[0] = 2;
+            fi[0] = 0;
+            nf = 1;
+        }
+    } else {
+        uint64_t wused = 0, bused = 0;
+        for (int e = 0; e < n_list; ++e) {
+            const uint32_t key = list[e].key;
+            const int kind = bp_kind(key);
+            if (kind == 2) {
+                const int sid = bp_static(key);
+                const int tag = sid >= 0 ? 100 + sid : -1;
+                const int body = bp_body_a(key);
+                for (int r = 0; r < wn; ++r) {
+                    if ((wused >> r) & 1ull) continue;
+                    if (cr.vel[r].body != body || cr.vel[r].tag != tag) continue;
+                    wused |= 1ull << r;
+                    nb[nn] = 0;
+                    ni[nn++] = static_cast<uint8_t>(r);
+                }
+            } else if (kind == 0 && bp_static(key) == kBpPredictiveId) {
+                for (int r = 0; r < bn; ++r) {
+                    if (((bused >> r) & 1ull) || !br.vel[r].predictive) continue;
+                    bused |= 1ull << r;
+                    nb[nn] = 2;
+                    ni[nn++] = static_cast<uint8_t>(r);
+                }
+            }
+        }
+        for (int r = 0; r < wn; ++r)
+            if (!((wused >> r) & 1ull)) {
+                nb[nn] = 0;
+                ni[nn++] = static_cast<uint8_t>(r);
+            }
+        for (int r = 0; r < bn; ++r)
+            if (!((bused >> r) & 1ull)) {
+                nb[nn] = 2;
+                ni[nn++] = static_cast<uint8_t>(r);
+            }
+        uint64_t wfu = 0, bfu = 0;
+        for (int k = 0; k < nn; ++k) {
+            if (nb[k] == 0) {
+                for (int f = 0; f < wf; ++f)
+                    if (!((wfu >> f) & 1ull) && cr.fric[f].normal_row == ni[k]) {
+                        wfu |= 1ull << f;
+                        fb[nf] = 0;
+                        fi[nf++] = static_cast<uint8_t>(f);
+                    }
+            } else {
+                for (int f = 0; f < bf; ++f)
+                    if (!((bfu >> f) & 1ull) && br.fric[f].normal_row == ni[k]) {
+                        bfu |= 1ull << f;
+                        fb[nf] = 2;
+                        fi[nf++] = static_cast<uint8_t>(f);
+                    }
+            }
+        }
+        for (int f = 0; f < wf; ++f)
+            if (!((wfu >> f) & 1ull)) {
+                fb[nf] = 0;
+                fi[nf++] = static_cast<uint8_t>(f);
+            }
+        for (int f = 0; f < bf; ++f)
+            if (!((bfu >> f) & 1ull)) {
+                fb[nf] = 2;
+                fi[nf++] = static_cast<uint8_t>(f);
+            }
+    }
+    // one normal / friction row against its body's accumulated velocity change
+    auto solve_normal = [](V3 normal, V3 rel_cross, V3 ang, float inv_mass, float jac, float rhs, float& applied,
+                           V3& dl, V3& da) {
+        float di = rhs;
+        const float dv = bt_dot(normal, dl) + bt_dot(rel_cross, da);
+        di = di - dv * jac;
+        const float before = applied;
+        const float sum = before + di;
+        if (sum < 0.0f) {
+            di = -before;
+            applied = 0.0f;
+        } else {
+            applied = sum;
+        }
+        if (di == 0.0f) return f2u(before) != f2u(applied);
+        dl = dl + (normal * inv_mass) * di;
+        da = da + ang * di;
+        return true;
+    };
+    auto solve_friction = [](V3 tangent, V3 rel_cross, V3 ang, float inv_mass, float jac, float rhs, float maxi,
+                             float& applied, V3& dl, V3& da) {
+        float di = rhs;
+        const float dv = bt_dot(tangent, dl) + bt_dot(rel_cross, da);
+        di = di - dv * jac;
+        const float before = applied;
+        const float sum = before + di;
+        if (sum < -maxi) {
+            di = -maxi - before;
+            applied = -maxi;
+        } else if (sum > maxi) {
+            di = maxi - before;
+            applied = maxi;
+        } else {
+            applied = sum;
+        }
+        if (di == 0.0f) return f2u(before) != f2u(applied);
+        dl = dl + (tangent * inv_mass) * di;
+        da = da + ang * di;
+        return true;
+    };
+    for (int iter = 0; iter < 10; ++iter) {
+        bool changed = false;
+        for (int k = 0; k < nn; ++k) {
+            if (nb[k] == 2) {
+                BallVelRow& r = br.vel[ni[k]];
+                changed = solve_normal(r.normal, r.rel_cross, r.ang, r.inv_mass, r.jac_inv, r.rhs, r.applied, ball_dl,
+                                       ball_da) || changed;
+            } else {
+                CarVelRow& r = cr.vel[ni[k]];
+                changed = solve_normal(r.normal, r.rel_cross, r.ang, r.inv_mass, r.jac, r.rhs, r.applied,
+                                       car_dl[r.body], car_da[r.body]) || changed;
+            }
+        }
+        for (int k = 0; k < nf; ++k) {
+            if (fb[k] == 2) {
+                BallFricRow& r = br.fric[fi[k]];
+                const float total = br.vel[r.normal_row].applied;
+                if (total <= 0.0f) continue;
+                changed = solve_friction(r.tangent, r.rel_cross, r.ang, r.inv_mass, r.jac_inv, r.rhs,
+                                         r.friction * total, r.applied, ball_dl, ball_da) || changed;
+            } else {
+                CarFricRow& r = cr.fric[fi[k]];
+                const float total = cr.vel[r.normal_row].applied;
+                if (total <= 0.0f) continue;
+                changed = solve_friction(r.tangent, r.rel_cross, r.ang, r.inv_mass, r.jac, r.rhs, r.friction * total,
+                                         r.applied, car_dl[r.body], car_da[r.body]) || changed;
+            }
+        }
+        if (!changed) break;
+    }
+}
+
+// Split-impulse position correction over the arena's penetration rows, ordered like the velocity rows
+// (reference SolveUnifiedSplitContactRows, arena_geometry.hpp:5035-5275). Returns the ball's push velocity; the cars'
+// push and turn velocities come back in `car_push` / `car_turn`, `car_bt` telling which cars had Bullet-unit rows.
+RG_HDI V3 unified_split_solve(BallContactRows& br, CarWorldRows& cr, const BpEntry* list, int n_list, V3* car_push,
+                              V3* car_turn, bool* car_bt, int count) {
+    constexpr int kMax = kMaxBallSplitRows + kMaxCarWorldRows;
+    for (int i = 0; i < count; ++i) car_bt[i] = false;
+    for (int r = 0; r < cr.ns; ++r) car_bt[cr.split[r].body] = true;
+    const int ws = cr.ns, bs = br.split_count;
+    uint8_t ob[kMax], oi[kMax];
+    int no = 0;
+    if (n_list > 0 && ws + bs > 1) {
+        uint64_t wused = 0, bused = 0;
+        for (int e = 0; e < n_list; ++e) {
+            const uint32_t key = list[e].key;
+            const int kind = bp_kind(key);
+            if (kind == 2) {
+                const int sid = bp_static(key);
+                const int tag = sid >= 0 ? 100 + sid : -1;
+                const int body = bp_body_a(key);
+                for (int r = 0; r < ws; ++r) {
+                    if (((wused >> r) & 1ull) || cr.split[r].body != body || cr.split[r].tag != tag) continue;
+                    wused |= 1ull << r;
+                    ob[no] = 0;
+                    oi[no++] = static_cast<uint8_t>(r);
+                }
+            } else if (kind == 0) {
+                for (int r = 0; r < bs; ++r) {
+                    if (((bused >> r) & 1ull) || br.split[r].static_id < 0 ||
+                        br.split[r].static_id != bp_static(key))
+                        continue;
+                    bused |= 1ull << r;
+                    ob[no] = 2;
+                    oi[no++] = static_cast<uint8_t>(r);
+                }
+            }
+        }
+        for (int r = 0; r < ws; ++r)
+            if (!((wused >> r) & 1ull)) {
+                ob[no] = 0;
+                oi[no++] = static_cast<uint8_t>(r);
+            }
+        for (int r = 0; r < bs; ++r)
+            if (!((bused >> r) & 1ull)) {
+                ob[no] = 2;
+                oi[no++] = static_cast<uint8_t>(r);
+            }
+    } else {
+        for (int r = 0; r < ws; ++r) {
+            ob[no] = 0;
+            oi[no++] = static_cast<uint8_t>(r);
+        }
+        for (int r = 0; r < bs; ++r) {
+            ob[no] = 2;
+            oi[no++] = static_cast<uint8_t>(r);
+        }
+    }
+    V3 push{0, 0, 0}, turn{0, 0, 0};
+    for (int i = 0; i < count; ++i) car_push[i] = car_turn[i] = V3{0.0f, 0.0f, 0.0f};
+    for (int iter = 0; iter < 10; ++iter) {
+        bool changed = false;
+        for (int k = 0; k < no; ++k) {
+            if (ob[k] == 2) {
+                BallSplitRow& r = br.split[oi[k]];
+                const float before = r.applied_bt;
+                float di = r.rhs_bt;
+                const float term = (bt_dot(r.normal, push) + bt_dot(r.rel_cross_bt, turn)) * r.jac_inv_bt;
+                di -= term;
+                const float sum = r.applied_bt + di;
+                if (sum < 0.0f) {
+                    di = -r.applied_bt;
+                    r.applied_bt = 0.0f;
+                } else {
+                    r.applied_bt = sum;
+                }
+                if (di == 0.0f) {
+                    changed = (f2u(before) != f2u(r.applied_bt)) || changed;
+                    continue;
+                }
+                push = push + (r.normal * r.inv_mass) * di;
+                turn = turn + r.ang_bt * di;
+                changed = true;
+            } else {
+                CarSplitRow& r = cr.split[oi[k]];
+                if (r.rhs == 0.0f) continue;
+                V3& p = car_push[r.body];
+                V3& t = car_turn[r.body];
+                const float before = r.applied;
+                float di = r.rhs;
+                di -= (bt_dot(r.normal, p) + bt_dot(r.rel_cross, t)) * r.jac;
+                const float sum = r.applied + di;
+                if (sum < 0.0f) {
+                    di = 0.0f - r.applied;
+                    r.applied = 0.0f;
+                } else {
+                    r.applied = sum;
+                }
+                if (di != 0.0f) {
+                    p = p + (r.normal * r.inv_mass) * di;
+                    t = t + r.ang * di;
+                }
+                changed = di != 0.0f || f2u(before) != f2u(r.applied) || changed;
+            }
+        }
+        if (!changed) break;
+    }
+    return push;
+}
+
+// One arena's world step with cars (reference WorldStepSoccar, env_step.hpp:4727-5623, on the path a custom-mesh
+// soccar arena takes): predictive rays, the broadphase's manifold list, the ball's and the cars' arena contacts, the
+// unified velocity and position solves, then integration. Car/ball and car/car contacts are not built yet: a pair
+// of bodies whose boxes meet only shapes the manifold list here.
+RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
+                            const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A, PreContactCar* pre,
+                            const TickSnap& snap) {
+    const int count = A.count;
+    const float sub_dt = c.tick_dt;
+    const bool vehicle_woke = (b.sleeping & 4u) != 0;
+    b.sleeping &= 3u;
+    const bool ball_sleeping = ball_resolve_activation(b);
+    if (vehicle_woke) b.deactivation_time = 0.0f;
+    const V3 ext_delta = ball_sleeping ? V3{0.0f, 0.0f, 0.0f} : V3{0.0f, 0.0f, c.gravity_z * sub_dt};
+    for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, sub_dt, pre[i]);
+    const V3 solver_vel_bt = b.vel_bt;
+    const bool awake = !ball_sleeping || vehicle_woke;
+    // predictive contacts (reference ComputePredictiveContactHits, env_step.hpp:4129-4168)
+    const int body_count = count + 1 < kBpBodies ? count + 1 : kBpBodies;
+    uint32_t pred_mask = 0u;
+    V3 pred_n[kBpBodies];
+    float pred_d[kBpBodies];
+    if (!(ball_sleeping && !vehicle_woke) && ball_predictive_hit(b, mesh, sub_dt, pred_n[0], pred_d[0])) pred_mask |= 1u;
+    for (int i = 0; i + 1 < body_count; ++i) {
+        if (pre[i].is_demoed) continue;
+        if (car_predictive_hit(A.cars[i], A.cfgs[i], mesh, sub_dt, pred_n[i + 1], pred_d[i + 1]))
+            pred_mask |= 1u << (i + 1);
+    }
+    // broadphase proxies and the manifold list (reference BuildBulletManifoldList + SortBulletManifoldListByIsland)
+    BpProxy proxies[kBpBodies];
+    ball_proxy(proxies[0], b.pos_bt, snap.ball_vel_bt, c.ball_radius, sub_dt);
+    for (int i = 0; i + 1 < body_count; ++i) {
+        BpProxy& p = proxies[i + 1];
+        const CarState& car = A.cars[i];
+        if (pre[i].is_demoed) {
+            p.valid = 0;
+            continue;
+        }
+        V3 ax = car.basis_forward, ay = car.basis_right, az = car.basis_up;
+        V3 px = ax, py = ay, pz = az;
+        Q4 unused{};
+        game_integrate_orientation(px, py, pz, unused, snap.car_ang_vel[i], sub_dt);
+        car_proxy(p, car.pos_bt, ax, ay, az, px, py, pz, snap.car_vel_bt[i], A.cfgs[i].hitbox_offset * (1.0f / 50.0f),
+                  car_box_half_bt(A.cfgs[i]), sub_dt);
+    }
+    BpEntry list[kBpMaxEntries];
+    const int n_list = bp_build_manifold_list(bp, proxies, body_count, mesh.aabb_min, mesh.aabb_max, pred_mask,
+                                              ball_sleeping && !vehicle_woke, list);
+    // the ball's arena contacts
+    BallContactRows rows;
+    rows.split_count = rows.vel_count = rows.fric_count = 0;
+    if (awake) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
+    // the cars' arena contacts, in slot order
+    CarWorldRows cr;
+    cr.nv = cr.nf = cr.ns = 0;
+    for (int i = 0; i < count; ++i) {
+        CarState& car = A.cars[i];
+        if (pre[i].is_demoed || car.just_respawned) {
+            cws[i].count = 0;
+            continue;
+        }
+        bool listed = false;
+        for (int e = 0; e < n_list; ++e) {
+            const uint32_t key = list[e].key;
+            listed = listed || (bp_kind(key) == 2 && bp_body_a(key) == i && bp_static(key) == 0);
+        }
+        if (!listed && cws[i].count == 0) continue;
+        const CarWorldContactResult res = car_mesh_contacts(car, A.cfgs[i], cws[i], listed, mesh, c, i, cr);
+        if (res.hit) {
+            car.world_contact.has_contact = 1;
+            car.world_contact.contact_normal = res.latest_normal;
+        }
+    }
+    // predictive rows, in the list's predictive order (reference AppendPredictiveContactRows)
+    for (int k = 0; k < bp.predictive_count; ++k) {
+        const uint32_t key = bp.predictive[k];
+        const int body = bp_entry_body(key);
+        if (((pred_mask >> body) & 1u) == 0u) continue;
+        if (body == 0) {
+            ball_predictive_rows(b, c, pred_n[0], pred_d[0], ext_delta, solver_vel_bt, sub_dt, rows);
+            continue;
+        }
+        const int i = body - 1;
+        const CarState& car = A.cars[i];
+        const V3 zero{0.0f, 0.0f, 0.0f};
+        const V3 n = pred_n[body];
+        const V3 tangent = contact_tangent(n, car.vel_bt + car.ext_force_impulse_bt);
+        car_contact_rows(cr, i, 100 + kBpPredictiveId, car, n, zero, pred_d[body], zero, zero, tangent, zero,
+                         1.0f / c.car_mass, 0.0f, c.arena_friction, sub_dt);
+    }
+    // a car with a predictive contact takes the game normal of all its arena rows (reference
+    // ApplyPredictiveCarWorldContactNormal, arena_ball.hpp:168-205)
+    for (int i = 0; i < count && i < 8; ++i) {
+        if (((pred_mask >> (i + 1)) & 1u) == 0u || !A.cars[i].world_contact.has_contact) continue;
+        V3 sum{0.0f, 0.0f, 0.0f};
+        bool any = false;
+        for (int pass = 0; pass < 2; ++pass) {
+            const int tag = pass == 0 ? 100 : 100 + kBpPredictiveId;
+            for (int r = 0; r < cr.nv; ++r) {
+                if (cr.vel[r].body != i || cr.vel[r].tag != tag) continue;
+                sum += cr.vel[r].normal;
+                any = true;
+            }
+        }
+        const float l2 = dot(sum, sum);
+        if (any && l2 >= 1e-8f) {
+            const V3 nn = sum * (1.0f / sqrtf(l2));
+            A.cars[i].world_contact.contact_normal = V3{0.0f + nn.x, 0.0f + nn.y, 0.0f + nn.z};
+        }
+    }
+    // velocity solve
+    if (rows.vel_count || rows.fric_count || cr.nv || cr.nf) {
+        V3 dl{0, 0, 0}, da{0, 0, 0};
+        V3 cdl[8], cda[8];
+        for (int i = 0; i < count; ++i) cdl[i] = cda[i] = V3{0.0f, 0.0f, 0.0f};
+        unified_velocity_solve(rows, cr, list, n_list, dl, da, cdl, cda);
+        ball_set_vel_bt(b, solver_vel_bt + dl);
+        b.ang_vel = b.ang_vel + da;
+        for (int i = 0; i < count; ++i) {
+            car_set_vel_bt(A.cars[i], A.cars[i].vel_bt + cdl[i]);
+            A.cars[i].ang_vel = A.cars[i].ang_vel + cda[i];
+        }
+    }
+    // position (split-impulse) solve
+    if (rows.split_count || cr.ns) {
+        V3 cpush[8], cturn[8];
+        bool cbt[8];
+        const V3 push = unified_split_solve(rows, cr, list, n_list, cpush, cturn, cbt, count);
+        if (!is_zero(push)) ball_set_pos_bt(b, b.pos_bt + push * sub_dt);
+        for (int i = 0; i < count; ++i) {
+            CarState& car = A.cars[i];
+            const bool nonzero = !is_zero(cpush[i]) || !is_zero(cturn[i]);
+            bool turn;
+            if (cbt[i]) {
+                turn = nonzero;
+                if (nonzero) car_set_pos_bt(car, car.pos_bt + cpush[i] * sub_dt);
+            } else {
+                turn = len2(cturn[i]) > 0.0f;
+                car_set_pos_bt(car, car.pos_bt + uu_to_bt_div(cpush[i]) * sub_dt);
+            }
+            if (turn)
+                game_integrate_orientation(car.basis_forward, car.basis_right, car.basis_up, car.rot,
+                                           cturn[i] * 0.1f, sub_dt);
+        }
+    }
+    // the ball's gravity, integration and deactivation clock
+    if (!ball_sleeping) ball_set_vel_bt(b, b.vel_bt + uu_to_bt_div(ext_delta));
+    if (awake) {
+        ball_integrate(b, sub_dt);
+        b.sleeping = 0;
+        const bool below = len2(b.vel_bt) < kBallLinearSleepBt * kBallLinearSleepBt &&
+                           len2(b.ang_vel) < kBallAngularSleep * kBallAngularSleep;
+        b.deactivation_time = below && !ball_sleeping ? b.deactivation_time + sub_dt : 0.0f;
+    }
+    for (int i = 0; i < count; ++i) car_world_finish(A.cars[i], pre[i], sub_dt);
+}
+
+// One tick of one arena with cars (reference StepEnvGeneric, env_step.hpp:7088-7180).
+RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
+                            const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
+                            const PadLayout& pads_layout, bool report_fields) {
     const int count = A.count;
     update_game_visit_order(env, A.cars, count);
     env.goal_scored_this_tick = 0;
     int order[8];
+    TickSnap snap;
     for (int k = 0; k < count; ++k) order[k] = car_visit_slot(env, k, count);
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         car_pre_tick(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i]);
+        if (i < 8) {
+            snap.car_vel_bt[i] = A.cars[i].vel_bt;
+            snap.car_ang_vel[i] = A.cars[i].ang_vel;
+        }
     }
     ball_tick_start_quantize(b, c);
     ball_clamp_and_drag(b, c);
+    snap.ball_vel_bt = b.vel_bt;
     if (c.enable_boost_pads && count > 0 && A.pads)
         for (int p = 0; p < pads_layout.count; ++p) pad_pre_tick(A.pads[p], c.tick_dt);
     for (int k = 0; k < count; ++k) {
@@ -357,9 +823,7 @@ RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, co
         vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh);
     }
     PreContactCar pre[8];
-    for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, c.tick_dt, pre[i]);
-    ball_world_step(b, s, c, mesh);
-    for (int i = 0; i < count; ++i) car_world_finish(A.cars[i], pre[i], c.tick_dt);
+    world_step_cars(b, s, bp, cws, c, mesh, A, pre, snap);
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         CarState& car = A.cars[i];

