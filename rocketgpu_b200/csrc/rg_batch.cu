@@ -88,6 +88,7 @@ struct rg_batch {
     DeviceArray<uint8_t> teams;
     DeviceArray<rg::Broadphase> broadphase;    // per arena: sweep history and manifold list
     DeviceArray<rg::CarWorldScratch> car_world;  // per car slot: the car/mesh manifold
+    DeviceArray<rg::BallCarScratch> ball_car;     // per car slot: the car/ball manifold
     rg::PadLayout pad_layout{};
     // Pads stay at their initial state until a car exists or pads are uploaded; until then ball-only arenas skip them.
     bool pads_live = false;
@@ -195,6 +196,7 @@ struct CarTickArgs {
     rg::PadLayout pad_layout;
     rg::Broadphase* broadphase;
     rg::CarWorldScratch* car_world;
+    rg::BallCarScratch* ball_car;
 };
 
 // Arenas with cars: ball, env and manifold scratch in registers as in tick_kernel; cars, wheel records and pads are
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(32) car_tick_kernel(CarTickArgs a, int ticks) 
     A.car_base = car_base;
     for (int t = 0; t < ticks; ++t) {
         A.controls = a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base;
-        rg::arena_tick_cars(env, b, s, a.broadphase[e], a.car_world + car_base, a.base.tc, a.base.mesh, A,
+        rg::arena_tick_cars(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc, a.base.mesh, A,
                             a.pad_layout, t + 1 == ticks);
     }
     a.base.balls[e] = b;
@@ -243,6 +245,7 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     a.pad_layout = b->pad_layout;
     a.broadphase = b->broadphase.ptr;
     a.car_world = b->car_world.ptr;
+    a.ball_car = b->ball_car.ptr;
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
     car_tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
@@ -257,7 +260,10 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
     // the reference resets the arena's whole solver scratch (src/rocketgpu.cpp:2107-2111): broadphase history,
     // manifold list and retained car manifolds start over
     memset(&a.broadphase[e], 0, sizeof(rg::Broadphase));
-    for (int k = 0; k < a.max_cars; ++k) a.car_world[car_base + k].count = 0;
+    for (int k = 0; k < a.max_cars; ++k) {
+        a.car_world[car_base + k].count = 0;
+        a.ball_car[car_base + k].count = 0;
+    }
     rg::reset_env_to_kickoff(e, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
                              a.car_cfgs + car_base, controls + car_base,
                              a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
@@ -283,6 +289,7 @@ void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
     a.pad_layout = b->pad_layout;
     a.broadphase = b->broadphase.ptr;
     a.car_world = b->car_world.ptr;
+    a.ball_car = b->ball_car.ptr;
     reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed);
     check(cudaGetLastError(), "reset_kickoff_kernel launch");
 }
@@ -496,6 +503,8 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         check(cudaMemset(b->broadphase.ptr, 0, b->env_count * sizeof(rg::Broadphase)), "broadphase");
         b->car_world.alloc(cap);
         if (cap) check(cudaMemset(b->car_world.ptr, 0, cap * sizeof(rg::CarWorldScratch)), "car manifolds");
+        b->ball_car.alloc(cap);
+        if (cap) check(cudaMemset(b->ball_car.ptr, 0, cap * sizeof(rg::BallCarScratch)), "car-ball manifolds");
         if (cap) {
             rg_car_state c0;
             rg_default_car_state(&c0);

@@ -77,17 +77,19 @@ RG_HD V3 inv_xform(const Xform& t, V3 v) {
 }
 
 // ---- shapes: a box (half extents without margin + margin) and a triangle -----------------------------------------
+enum ShapeKind : uint8_t { kTriangle = 0, kBox = 1, kSphere = 2 };
 struct Shape {
-    uint8_t is_box;
+    uint8_t kind;
     V3 half;      // box: implicit dimensions
     V3 v[3];      // triangle vertices
-    float margin;
+    float margin; // sphere: the radius
 };
 RG_HD V3 support_no_margin(const Shape& s, V3 d) {
-    if (s.is_box) {
+    if (s.kind == kBox) {
         return V3{d.x >= 0.0f ? s.half.x : -s.half.x, d.y >= 0.0f ? s.half.y : -s.half.y,
                   d.z >= 0.0f ? s.half.z : -s.half.z};
     }
+    if (s.kind == kSphere) return V3{0.0f, 0.0f, 0.0f};
     const V3 dots{bdot(d, s.v[0]), bdot(d, s.v[1]), bdot(d, s.v[2])};
     const int ax = dots.x < dots.y ? (dots.y < dots.z ? 2 : 1) : (dots.x < dots.z ? 2 : 0);
     return s.v[ax];
@@ -101,7 +103,7 @@ RG_HD V3 support_margin(const Shape& s, V3 d) {
 // The reference's box shape from half extents with the margin included (MakeBulletPortBoxShape).
 RG_HDI Shape make_box(V3 half_with_margin, float margin) {
     Shape s;
-    s.is_box = 1;
+    s.kind = kBox;
     const float min_dim = fmin_(half_with_margin.x, fmin_(half_with_margin.y, half_with_margin.z));
     const float safe_margin = fmin_(margin, 0.1f * min_dim);
     s.half = half_with_margin - V3{safe_margin, safe_margin, safe_margin};
@@ -109,9 +111,17 @@ RG_HDI Shape make_box(V3 half_with_margin, float margin) {
     s.v[0] = s.v[1] = s.v[2] = V3{0.0f, 0.0f, 0.0f};
     return s;
 }
+RG_HDI Shape make_sphere(float radius) {
+    Shape s;
+    s.kind = kSphere;
+    s.half = V3{0.0f, 0.0f, 0.0f};
+    s.v[0] = s.v[1] = s.v[2] = V3{0.0f, 0.0f, 0.0f};
+    s.margin = radius;
+    return s;
+}
 RG_HDI Shape make_triangle(V3 a, V3 b, V3 c) {
     Shape s;
-    s.is_box = 0;
+    s.kind = kTriangle;
     s.half = V3{0.0f, 0.0f, 0.0f};
     s.v[0] = a;
     s.v[1] = b;
@@ -1072,12 +1082,82 @@ RG_HDI Xform basis_xform(V3 f, V3 r, V3 u, V3 origin) {
     return t;
 }
 
+// Bullet's GJK pair detector loop between shape `a` (in `xa`) and `b` (in `xb`), without margins
+// (reference RunCarArenaTriangleGjkSimplex / RunBallCarGjkSimplex, triangle_and_carcar.hpp:206-300, 538-624):
+// iterates the Voronoi simplex toward the origin until a termination rule fires. Returns whether it ended on a rule
+// that yields closest points (`pa`, `pb`, world space); `degenerate` records which rule.
+RG_HDI bool pair_detector(const Shape& a, const Xform& xa, const Shape& b, const Xform& xb, float max_dist_sq,
+                          V3& cached_axis, int& degenerate, float& squared_distance, V3& pa, V3& pb) {
+    constexpr float kRelError2 = 1.0e-6f;
+    bool check_simplex = false;
+    VoronoiSimplex sx;
+    sx.reset();
+    int cur_iter = 0;
+    while (true) {
+        const V3 sep_a = vec_mul_mat(-cached_axis, xa.b);
+        const V3 sep_b = vec_mul_mat(cached_axis, xb.b);
+        const V3 pw = xform(xa, support_no_margin(a, sep_a));
+        const V3 qw = xform(xb, support_no_margin(b, sep_b));
+        const V3 w = pw - qw;
+        const float delta = dot(cached_axis, w);
+        if ((delta > 0.0f) && (delta * delta > squared_distance * max_dist_sq)) {
+            degenerate = 10;
+            check_simplex = true;
+            break;
+        }
+        if (sx.in_simplex(w)) {
+            degenerate = 1;
+            check_simplex = true;
+            break;
+        }
+        const float f0 = squared_distance - delta;
+        const float f1 = squared_distance * kRelError2;
+        if (f0 <= f1) {
+            degenerate = f0 <= 0.0f ? 2 : 11;
+            check_simplex = true;
+            break;
+        }
+        sx.add(w, pw, qw);
+        const bool ok = sx.update();
+        const V3 new_axis = sx.cv;
+        if (!ok) {
+            degenerate = 3;
+            check_simplex = true;
+            break;
+        }
+        if (len2(new_axis) < kRelError2) {
+            cached_axis = new_axis;
+            degenerate = 6;
+            check_simplex = true;
+            break;
+        }
+        const float prev = squared_distance;
+        squared_distance = len2(new_axis);
+        if (prev - squared_distance <= 1.1920929e-7f * prev) {
+            check_simplex = true;
+            degenerate = 12;
+            break;
+        }
+        cached_axis = new_axis;
+        if (cur_iter++ > 1000) break;
+        if (sx.full()) {
+            degenerate = 13;
+            break;
+        }
+    }
+    if (check_simplex) {
+        sx.update();
+        pa = sx.cp1;
+        pb = sx.cp2;
+    }
+    return check_simplex;
+}
+
 // Closest points / penetration of the car's hitbox (half extents `raw_half_bt`, Bullet margin 0.04) and a triangle
 // (reference ComputeCarArenaTriangleContact). Returns false when there is no contact within 10 bt; otherwise the
 // signed distance and the witness point on the triangle.
 RG_HDI bool box_triangle_contact(V3 basis_f, V3 basis_r, V3 basis_u, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt,
                                  V3 ta, V3 tb, V3 tc, float& out_distance_bt, V3& out_point_on_b_bt) {
-    constexpr float kRelError2 = 1.0e-6f;
     const Shape box = make_box(raw_half_bt, 0.04f);
     const Shape tri = make_triangle(ta, tb, tc);
     const float margin_a = box.margin, margin_b = tri.margin;
@@ -1100,72 +1180,8 @@ RG_HDI bool box_triangle_contact(V3 basis_f, V3 basis_r, V3 basis_u, V3 car_pos_
     V3 point_a{0.0f, 0.0f, 0.0f}, point_b{0.0f, 0.0f, 0.0f};
 
     // GJK pair-detector loop (RunCarArenaTriangleGjkSimplex)
-    bool check_simplex = false;
-    {
-        VoronoiSimplex sx;
-        sx.reset();
-        int cur_iter = 0;
-        while (true) {
-            const V3 sep_a = vec_mul_mat(-cached_axis, ta_x.b);
-            const V3 sep_b = vec_mul_mat(cached_axis, tb_x.b);
-            const V3 pa = support_no_margin(box, sep_a);
-            const V3 qb = support_no_margin(tri, sep_b);
-            const V3 pw = xform(ta_x, pa);
-            const V3 qw = xform(tb_x, qb);
-            const V3 w = pw - qw;
-            const float delta = dot(cached_axis, w);
-            const bool in_sx = sx.in_simplex(w);
-            const float f0 = squared_distance - delta;
-            const float f1 = squared_distance * kRelError2;
-            if ((delta > 0.0f) && (delta * delta > squared_distance * 100.0f)) {
-                degenerate = 10;
-                check_simplex = true;
-                break;
-            }
-            if (in_sx) {
-                degenerate = 1;
-                check_simplex = true;
-                break;
-            }
-            if (f0 <= f1) {
-                degenerate = f0 <= 0.0f ? 2 : 11;
-                check_simplex = true;
-                break;
-            }
-            sx.add(w, pw, qw);
-            const bool ok = sx.update();
-            const V3 new_axis = sx.cv;
-            if (!ok) {
-                degenerate = 3;
-                check_simplex = true;
-                break;
-            }
-            if (len2(new_axis) < kRelError2) {
-                cached_axis = new_axis;
-                degenerate = 6;
-                check_simplex = true;
-                break;
-            }
-            const float prev = squared_distance;
-            squared_distance = len2(new_axis);
-            if (prev - squared_distance <= 1.1920929e-7f * prev) {
-                check_simplex = true;
-                degenerate = 12;
-                break;
-            }
-            cached_axis = new_axis;
-            if (cur_iter++ > 1000) break;
-            if (sx.full()) {
-                degenerate = 13;
-                break;
-            }
-        }
-        if (check_simplex) {
-            sx.update();
-            point_a = sx.cp1;
-            point_b = sx.cp2;
-        }
-    }
+    const bool check_simplex =
+        pair_detector(box, ta_x, tri, tb_x, 100.0f, cached_axis, degenerate, squared_distance, point_a, point_b);
     if (check_simplex) {
         const float l2 = len2(cached_axis);
         if (l2 <= 0.0001f) degenerate = 5;
@@ -1230,6 +1246,136 @@ RG_HDI bool box_triangle_contact(V3 basis_f, V3 basis_r, V3 basis_u, V3 car_pos_
     point_b = point_b + offset;
     out_distance_bt = distance_bt;
     out_point_on_b_bt = point_b;
+    return true;
+}
+
+// ---- box vs sphere ---------------------------------------------------------------------------------------------
+// World AABB centre of a box or sphere under `t` (btConvexShape::getAabb), as the normal-direction fix reads it.
+RG_HDI V3 aabb_center(const Shape& s, const Xform& t) {
+    if (s.kind == kBox) {
+        const V3 h = s.half + V3{s.margin, s.margin, s.margin};
+        const V3 a0{fabs_(t.b.r[0].x), fabs_(t.b.r[0].y), fabs_(t.b.r[0].z)};
+        const V3 a1{fabs_(t.b.r[1].x), fabs_(t.b.r[1].y), fabs_(t.b.r[1].z)};
+        const V3 a2{fabs_(t.b.r[2].x), fabs_(t.b.r[2].y), fabs_(t.b.r[2].z)};
+        const V3 e{bdot(h, a0), bdot(h, a1), bdot(h, a2)};
+        return ((t.o + e) + (t.o - e)) * 0.5f;
+    }
+    const V3 e{s.margin, s.margin, s.margin};
+    return ((t.o + e) + (t.o - e)) * 0.5f;
+}
+
+struct BallBoxContact {
+    V3 normal;          // from the car toward the ball
+    float distance_bt;  // signed separation
+    V3 rel_ball_bt, rel_car_bt;    // contact points relative to the ball / car origins
+    V3 ball_local_bt, car_local_bt;  // the same points in the bodies' frames
+};
+// The car's hitbox (raw half extents, Bullet margin 0.04) against the ball's sphere (reference
+// ComputeBallCarContactGeometryGjk, triangle_and_carcar.hpp:626-821): the GJK pair detector, EPA when they overlap,
+// the contact kept within the breaking threshold. False leaves the caller to the sphere-box fallback.
+RG_HDI bool ball_box_contact(V3 cf, V3 cr, V3 cu, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt, V3 bx, V3 by,
+                             V3 bz, V3 ball_pos_bt, float radius_bt, float threshold_bt, BallBoxContact& out) {
+    const Shape box = make_box(raw_half_bt, 0.04f);
+    const Shape sphere = make_sphere(radius_bt);
+    const float margin_a = box.margin, margin_b = sphere.margin;
+    float max_dist_sq = margin_a + margin_b + threshold_bt;
+    max_dist_sq *= max_dist_sq;
+    Xform xa = basis_xform(cf, cr, cu, car_pos_bt);
+    xa.o = xform(xa, child_offset_bt);
+    Xform xb = basis_xform(bx, by, bz, ball_pos_bt);
+    const V3 offset = (xa.o + xb.o) * 0.5f;
+    xa.o = xa.o - offset;
+    xb.o = xb.o - offset;
+    V3 cached_axis{0.0f, 1.0f, 0.0f};
+    float squared_distance = 1.0e30f;
+    bool is_valid = false;
+    int degenerate = 0;
+    float distance_bt = 0.0f;
+    V3 normal{0.0f, 0.0f, 0.0f}, pa{0.0f, 0.0f, 0.0f}, pb{0.0f, 0.0f, 0.0f};
+    if (!pair_detector(box, xa, sphere, xb, max_dist_sq, cached_axis, degenerate, squared_distance, pa, pb))
+        return false;
+    const float len_sqr = len2(cached_axis);
+    if (len_sqr <= 0.0001f) degenerate = 5;
+    const float s = sqrtf(squared_distance);
+    if (len_sqr > 1.1920929e-7f * 1.1920929e-7f) {
+        const float inv_len = 1.0f / sqrtf(len_sqr);
+        normal = cached_axis * inv_len;
+        if (s > 0.0f) {
+            pa = pa - cached_axis * (margin_a / s);
+            pb = pb + cached_axis * (margin_b / s);
+            distance_bt = (1.0f / inv_len) - (margin_a + margin_b);
+            is_valid = true;
+        }
+    }
+    const bool catch_degenerate = degenerate && ((distance_bt + (margin_a + margin_b)) <= 0.01f);
+    if (!is_valid || catch_degenerate) {
+        const V3 delta_origin = xb.o - xa.o;
+        const float dl2 = blen2(delta_origin);
+        const V3 guess = dl2 > 1.0e-20f ? bdiv(delta_origin, sqrtf(dl2)) : V3{0.0f, 0.0f, 0.0f};
+        Results r;
+        V3 sep{0.0f, 0.0f, 0.0f}, wa{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
+        bool pen = false;
+        if (penetration(box, xa, sphere, xb, guess, r)) {
+            wa = r.witness0;
+            wb = r.witness1;
+            sep = r.normal;
+            pen = true;
+        } else if (distance(box, xa, sphere, xb, guess, r)) {
+            wa = r.witness0;
+            wb = r.witness1;
+            sep = r.normal;
+        }
+        if (pen) {
+            V3 nb = wb - wa;
+            float l2 = blen2(nb);
+            if (l2 <= 1.1920929e-7f * 1.1920929e-7f) {
+                nb = sep;
+                l2 = blen2(sep);
+            }
+            if (l2 > 1.1920929e-7f * 1.1920929e-7f) {
+                nb = bdiv(nb, sqrtf(l2));
+                const float d2 = -len(wa - wb);
+                if (!is_valid || d2 < distance_bt) {
+                    distance_bt = d2;
+                    pa = wa;
+                    pb = wb;
+                    normal = nb;
+                    is_valid = true;
+                }
+            }
+        } else if (blen2(sep) > 0.0f) {
+            const float d2 = len(wa - wb) - (margin_a + margin_b);
+            if (!is_valid || d2 < distance_bt) {
+                pa = wa - sep * margin_a;
+                pb = wb + sep * margin_b;
+                const float l2 = dot(sep, sep);
+                normal = l2 <= 1e-12f ? normal : sep * (1.0f / sqrtf(l2));
+                distance_bt = d2;
+                is_valid = true;
+            }
+        }
+    }
+    if (!is_valid) return false;
+    if (!((distance_bt < 0.0f) || (distance_bt * distance_bt < max_dist_sq))) return false;
+    if (distance_bt > threshold_bt) return false;
+    const V3 point_on_ball = pb + offset;
+    // the normal made to point from the sphere toward the box (FixArenaTriangleContactNormalDirectionBullet)
+    const V3 diff = aabb_center(box, xa) - aabb_center(sphere, xb);
+    V3 bn = normal;
+    if (bdot(diff, bn) < 0.0f) bn = bn * -1.0f;
+    const V3 point_on_car = point_on_ball + bn * distance_bt;
+    out.normal = -bn;
+    out.distance_bt = distance_bt;
+    const V3 car_local = vec_mul_mat(point_on_car - car_pos_bt, xa.b);
+    const V3 ball_local = vec_mul_mat(point_on_ball - ball_pos_bt, xb.b);
+    const V3 car_ref = V3{bdot(car_local, xa.b.r[0]), bdot(car_local, xa.b.r[1]), bdot(car_local, xa.b.r[2])} +
+                       car_pos_bt;
+    const V3 ball_ref = V3{bdot(ball_local, xb.b.r[0]), bdot(ball_local, xb.b.r[1]), bdot(ball_local, xb.b.r[2])} +
+                        ball_pos_bt;
+    out.rel_ball_bt = ball_ref - ball_pos_bt;
+    out.rel_car_bt = car_ref - car_pos_bt;
+    out.ball_local_bt = ball_local;
+    out.car_local_bt = car_local;
     return true;
 }
 

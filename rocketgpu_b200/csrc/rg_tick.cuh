@@ -7,6 +7,7 @@
 // (env_step.hpp:4622-5623) and StepEnvTail (env_step.hpp:6968-7045).
 #pragma once
 
+#include "rg_ball_car.cuh"
 #include "rg_ball_world.cuh"
 #include "rg_broadphase.cuh"
 #include "rg_car_world.cuh"
@@ -308,7 +309,8 @@ RG_HDI void update_game_visit_order(EnvState& env, const CarState* cars, int cou
 // A car's tick start (reference StepEnvPreTickCar, env_step.hpp:6751-6873): working fields back from the report
 // fields, internal clocks after a state set, the demolition timer, the tick-start quantization, the pre-physics
 // control logic and the rigid-body speed clamp.
-RG_HDI void car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w) {
+// Returns the car's uu velocity right after the tick-start quantisation.
+RG_HDI V3 car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w) {
     c.ball_contact_this_tick = 0;
     restore_step_fields(c);
     if (c.tick_count_since_update == 0) cal_internal_timers_from_set_state(c, tc);
@@ -334,6 +336,7 @@ RG_HDI void car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg
         const bool impulsed = c.vel_bt.x != before.x || c.vel_bt.y != before.y || c.vel_bt.z != before.z;
         if ((car_body_damping_clamp(c, tc) & 1) && impulsed) car_set_vel_bt(c, c.vel_bt);
     }
+    return snap_vel;
 }
 
 // ---- the world step of an arena with cars ------------------------------------------------------------------------
@@ -342,6 +345,9 @@ RG_HDI void car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg
 struct TickSnap {
     V3 ball_vel_bt;
     V3 car_vel_bt[8], car_ang_vel[8];
+    // uu velocities right after the tick-start quantisation, for the ball-hit impulse (reference cal_start_vel /
+    // cal_ball_start_vel)
+    V3 car_start_vel[8], ball_start_vel;
 };
 
 // The car's predictive (CCD) contact: its box centre's motion this tick (reference PredictiveContactRayForBody
@@ -367,13 +373,20 @@ RG_HDI bool car_predictive_hit(const CarState& c, const CarConfig& cfg, const Me
 // PGS at the velocity level over every contact row of the arena, in the order the sorted manifold list gives
 // (reference SolveUnifiedVelocityContactRowsGeneral, arena_geometry.hpp:5527-5866): for each listed manifold its rows,
 // then the unlisted car rows, then the unlisted ball rows; each normal row's friction row follows the normal order.
-// Rows act on their own body's velocity deltas; one iteration count (stop when nothing changed) covers all.
-RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const BpEntry* list, int n_list,
-                                   V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
-    constexpr int kMax = kMaxBallVelRows + kMaxCarWorldRows;
+// The ball's rows are indexed car-ball rows first, then its arena rows, the order the world step appends them in.
+// Rows act on their bodies' velocity deltas (a car-ball row on both, reference
+// SolveBallVelocity{Normal,Friction}RowWithAccumulators, arena_geometry.hpp:2618-2750); one iteration count (stop
+// when nothing changed) covers all.
+RG_HDI void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list,
+                                   int n_list, V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
+    constexpr int kMax = kMaxBallVelRows + kMaxBallCarRows + kMaxCarWorldRows;
     uint8_t nb[kMax], ni[kMax], fb[kMax], fi[kMax];
     int nn = 0, nf = 0;
-    const int wn = cr.nv, bn = br.vel_count, wf = cr.nf, bf = br.fric_count;
+    const int bcn = bc.nv, bcf = bc.nf;
+    const int wn = cr.nv, bn = bcn + br.vel_count, wf = cr.nf, bf = bcf + br.fric_count;
+    // combined ball index: car-ball rows first
+    auto ball_fric_normal = [&](int f) { return f < bcf ? bc.fric[f].normal_row : br.fric[f - bcf].normal_row + bcn; };
+    auto ball_applied = [&](int r) { return r < bcn ? bc.vel[r].applied : br.vel[r - bcn].applied; };
     if (wn + bn <= 1 && wf + bf <= 1) {
         if (wn == 1) {
             nb[0] = 0;
@@ -409,9 +422,17 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const 
                     nb[nn] = 0;
                     ni[nn++] = static_cast<uint8_t>(r);
                 }
+            } else if (kind == 1) {
+                const int car = bp_body_a(key);
+                for (int r = 0; r < bcn; ++r) {
+                    if (((bused >> r) & 1ull) || bc.vel[r].car != car) continue;
+                    bused |= 1ull << r;
+                    nb[nn] = 2;
+                    ni[nn++] = static_cast<uint8_t>(r);
+                }
             } else if (kind == 0 && bp_static(key) == kBpPredictiveId) {
-                for (int r = 0; r < bn; ++r) {
-                    if (((bused >> r) & 1ull) || !br.vel[r].predictive) continue;
+                for (int r = bcn; r < bn; ++r) {
+                    if (((bused >> r) & 1ull) || !br.vel[r - bcn].predictive) continue;
                     bused |= 1ull << r;
                     nb[nn] = 2;
                     ni[nn++] = static_cast<uint8_t>(r);
@@ -439,7 +460,7 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const 
                     }
             } else {
                 for (int f = 0; f < bf; ++f)
-                    if (!((bfu >> f) & 1ull) && br.fric[f].normal_row == ni[k]) {
+                    if (!((bfu >> f) & 1ull) && ball_fric_normal(f) == ni[k]) {
                         bfu |= 1ull << f;
                         fb[nf] = 2;
                         fi[nf++] = static_cast<uint8_t>(f);
@@ -497,11 +518,63 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const 
         da = da + ang * di;
         return true;
     };
+    // a car-ball row: the car is Bullet's body 1 (direction -n), the ball body 2
+    auto solve_pair = [](V3 n, V3 rel_ball_cross, V3 ball_ang, float ball_inv, V3 rel_car_cross, V3 car_ang,
+                         float car_inv, float jac, float rhs, float lo, float hi, float& applied, V3& bdl, V3& bda,
+                         V3& cdl, V3& cda) {
+        float di = rhs;
+        const float dv1 = bt_dot(-n, cdl) + bt_dot(rel_car_cross, cda);
+        const float dv2 = bt_dot(n, bdl) + bt_dot(rel_ball_cross, bda);
+        di = di - dv1 * jac;
+        di = di - dv2 * jac;
+        const float before = applied;
+        const float sum = before + di;
+        if (sum < lo) {
+            di = lo - before;
+            applied = lo;
+        } else if (sum > hi) {
+            di = hi - before;
+            applied = hi;
+        } else {
+            applied = sum;
+        }
+        if (di == 0.0f) return f2u(before) != f2u(applied);
+        bdl = bdl + (n * ball_inv) * di;
+        bda = bda + ball_ang * di;
+        cdl = cdl + ((-n) * car_inv) * di;
+        cda = cda + car_ang * di;
+        return true;
+    };
     for (int iter = 0; iter < 10; ++iter) {
         bool changed = false;
         for (int k = 0; k < nn; ++k) {
-            if (nb[k] == 2) {
-                BallVelRow& r = br.vel[ni[k]];
+            if (nb[k] == 2 && ni[k] < bcn) {
+                BcVelRow& r = bc.vel[ni[k]];
+                // the normal row's lower clamp: sum < 0 -> di = -before, applied = 0
+                float di = r.rhs;
+                const float dv1 = bt_dot(-r.normal, car_dl[r.car]) + bt_dot(r.rel_car_cross, car_da[r.car]);
+                const float dv2 = bt_dot(r.normal, ball_dl) + bt_dot(r.rel_ball_cross, ball_da);
+                di = di - dv1 * r.jac;
+                di = di - dv2 * r.jac;
+                const float before = r.applied;
+                const float sum = before + di;
+                if (sum < 0.0f) {
+                    di = -before;
+                    r.applied = 0.0f;
+                } else {
+                    r.applied = sum;
+                }
+                if (di == 0.0f) {
+                    changed = (f2u(before) != f2u(r.applied)) || changed;
+                    continue;
+                }
+                ball_dl = ball_dl + (r.normal * r.ball_inv_mass) * di;
+                ball_da = ball_da + r.ball_ang * di;
+                car_dl[r.car] = car_dl[r.car] + ((-r.normal) * r.car_inv_mass) * di;
+                car_da[r.car] = car_da[r.car] + r.car_ang * di;
+                changed = true;
+            } else if (nb[k] == 2) {
+                BallVelRow& r = br.vel[ni[k] - bcn];
                 changed = solve_normal(r.normal, r.rel_cross, r.ang, r.inv_mass, r.jac_inv, r.rhs, r.applied, ball_dl,
                                        ball_da) || changed;
             } else {
@@ -511,9 +584,17 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const 
             }
         }
         for (int k = 0; k < nf; ++k) {
-            if (fb[k] == 2) {
-                BallFricRow& r = br.fric[fi[k]];
-                const float total = br.vel[r.normal_row].applied;
+            if (fb[k] == 2 && fi[k] < bcf) {
+                BcFricRow& r = bc.fric[fi[k]];
+                const float total = ball_applied(r.normal_row);
+                if (total <= 0.0f) continue;
+                const float maxi = r.friction * total;
+                changed = solve_pair(r.tangent, r.rel_ball_cross, r.ball_ang, r.ball_inv_mass, r.rel_car_cross,
+                                     r.car_ang, r.car_inv_mass, r.jac, r.rhs, -maxi, maxi, r.applied, ball_dl, ball_da,
+                                     car_dl[r.car], car_da[r.car]) || changed;
+            } else if (fb[k] == 2) {
+                BallFricRow& r = br.fric[fi[k] - bcf];
+                const float total = ball_applied(r.normal_row + bcn);
                 if (total <= 0.0f) continue;
                 changed = solve_friction(r.tangent, r.rel_cross, r.ang, r.inv_mass, r.jac_inv, r.rhs,
                                          r.friction * total, r.applied, ball_dl, ball_da) || changed;
@@ -530,14 +611,18 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, CarWorldRows& cr, const 
 }
 
 // Split-impulse position correction over the arena's penetration rows, ordered like the velocity rows
-// (reference SolveUnifiedSplitContactRows, arena_geometry.hpp:5035-5275). Returns the ball's push velocity; the cars'
-// push and turn velocities come back in `car_push` / `car_turn`, `car_bt` telling which cars had Bullet-unit rows.
-RG_HDI V3 unified_split_solve(BallContactRows& br, CarWorldRows& cr, const BpEntry* list, int n_list, V3* car_push,
-                              V3* car_turn, bool* car_bt, int count) {
-    constexpr int kMax = kMaxBallSplitRows + kMaxCarWorldRows;
+// (reference SolveUnifiedSplitContactRows, arena_geometry.hpp:5035-5275; car-ball rows as in
+// SolveUnifiedBallSplitRow, :3523-3600). Returns the ball's push velocity; the cars' push and turn velocities come
+// back in `car_push` / `car_turn`, `car_bt` telling which cars had Bullet-unit rows (every row here carries Bullet
+// units, so a car is in Bullet units when any of its arena or car-ball rows exists, MarkBtSplitAccumulators).
+RG_HDI V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list, int n_list,
+                              V3* car_push, V3* car_turn, bool* car_bt, int count) {
+    constexpr int kMax = kMaxBallSplitRows + kMaxBallCarRows + kMaxCarWorldRows;
     for (int i = 0; i < count; ++i) car_bt[i] = false;
     for (int r = 0; r < cr.ns; ++r) car_bt[cr.split[r].body] = true;
-    const int ws = cr.ns, bs = br.split_count;
+    for (int r = 0; r < bc.ns; ++r) car_bt[bc.split[r].car] = true;
+    const int bcs = bc.ns;
+    const int ws = cr.ns, bs = bcs + br.split_count;
     uint8_t ob[kMax], oi[kMax];
     int no = 0;
     if (n_list > 0 && ws + bs > 1) {
@@ -555,11 +640,18 @@ RG_HDI V3 unified_split_solve(BallContactRows& br, CarWorldRows& cr, const BpEnt
                     ob[no] = 0;
                     oi[no++] = static_cast<uint8_t>(r);
                 }
+            } else if (kind == 1) {
+                const int car = bp_body_a(key);
+                for (int r = 0; r < bcs; ++r) {
+                    if (((bused >> r) & 1ull) || bc.split[r].car != car) continue;
+                    bused |= 1ull << r;
+                    ob[no] = 2;
+                    oi[no++] = static_cast<uint8_t>(r);
+                }
             } else if (kind == 0) {
-                for (int r = 0; r < bs; ++r) {
-                    if (((bused >> r) & 1ull) || br.split[r].static_id < 0 ||
-                        br.split[r].static_id != bp_static(key))
-                        continue;
+                for (int r = bcs; r < bs; ++r) {
+                    const BallSplitRow& row = br.split[r - bcs];
+                    if (((bused >> r) & 1ull) || row.static_id < 0 || row.static_id != bp_static(key)) continue;
                     bused |= 1ull << r;
                     ob[no] = 2;
                     oi[no++] = static_cast<uint8_t>(r);
@@ -591,8 +683,33 @@ RG_HDI V3 unified_split_solve(BallContactRows& br, CarWorldRows& cr, const BpEnt
     for (int iter = 0; iter < 10; ++iter) {
         bool changed = false;
         for (int k = 0; k < no; ++k) {
-            if (ob[k] == 2) {
-                BallSplitRow& r = br.split[oi[k]];
+            if (ob[k] == 2 && oi[k] < bcs) {
+                BcSplitRow& r = bc.split[oi[k]];
+                V3& p = car_push[r.car];
+                V3& t = car_turn[r.car];
+                const float before = r.applied;
+                float di = r.rhs;
+                const float ball_term = (bt_dot(r.normal, push) + bt_dot(r.rel_ball_cross, turn)) * r.jac;
+                di -= (bt_dot(-r.normal, p) + bt_dot(r.rel_car_cross, t)) * r.jac;
+                di -= ball_term;
+                const float sum = r.applied + di;
+                if (sum < 0.0f) {
+                    di = -r.applied;
+                    r.applied = 0.0f;
+                } else {
+                    r.applied = sum;
+                }
+                if (di == 0.0f) {
+                    changed = (f2u(before) != f2u(r.applied)) || changed;
+                    continue;
+                }
+                push = push + (r.normal * r.ball_inv_mass) * di;
+                turn = turn + r.ball_ang * di;
+                p = p + ((-r.normal) * r.car_inv_mass) * di;
+                t = t + r.car_ang * di;
+                changed = true;
+            } else if (ob[k] == 2) {
+                BallSplitRow& r = br.split[oi[k] - bcs];
                 const float before = r.applied_bt;
                 float di = r.rhs_bt;
                 const float term = (bt_dot(r.normal, push) + bt_dot(r.rel_cross_bt, turn)) * r.jac_inv_bt;
@@ -640,11 +757,12 @@ RG_HDI V3 unified_split_solve(BallContactRows& br, CarWorldRows& cr, const BpEnt
 
 // One arena's world step with cars (reference WorldStepSoccar, env_step.hpp:4727-5623, on the path a custom-mesh
 // soccar arena takes): predictive rays, the broadphase's manifold list, the ball's and the cars' arena contacts, the
-// unified velocity and position solves, then integration. Car/ball and car/car contacts are not built yet: a pair
-// of bodies whose boxes meet only shapes the manifold list here.
+// unified velocity and position solves, then integration; car-ball contacts (reference env_step.hpp:5045-5133)
+// with their ball-hit bookkeeping. Car/car contacts are not built yet: two cars whose boxes meet only shape the
+// manifold list here.
 RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
-                            const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A, PreContactCar* pre,
-                            const TickSnap& snap) {
+                            BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
+                            PreContactCar* pre, const TickSnap& snap, uint64_t env_tick) {
     const int count = A.count;
     const float sub_dt = c.tick_dt;
     const bool vehicle_woke = (b.sleeping & 4u) != 0;
@@ -654,6 +772,14 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
     const V3 ext_delta = ball_sleeping ? V3{0.0f, 0.0f, 0.0f} : V3{0.0f, 0.0f, c.gravity_z * sub_dt};
     for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, sub_dt, pre[i]);
     const V3 solver_vel_bt = b.vel_bt;
+    // where the bodies stand at the step's start, for the ball-hit records (reference record_ball_car_info)
+    const V3 hit_ball_pos = b.pos;
+    V3 hit_car_pos[8];
+    Q4 hit_car_rot[8];
+    for (int i = 0; i < count && i < 8; ++i) {
+        hit_car_pos[i] = A.cars[i].pos;
+        hit_car_rot[i] = A.cars[i].rot;
+    }
     const bool awake = !ball_sleeping || vehicle_woke;
     // predictive contacts (reference ComputePredictiveContactHits, env_step.hpp:4129-4168)
     const int body_count = count + 1 < kBpBodies ? count + 1 : kBpBodies;
@@ -686,10 +812,35 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
     BpEntry list[kBpMaxEntries];
     const int n_list = bp_build_manifold_list(bp, proxies, body_count, mesh.aabb_min, mesh.aabb_max, pred_mask,
                                               ball_sleeping && !vehicle_woke, list);
-    // the ball's arena contacts
+    // car-ball contacts, in slot order: a car whose box AABB meets the ball's takes part (reference
+    // env_step.hpp:5045-5133; a car with no valid proxy is demolished and never overlaps,
+    // BallCarRetainedPairOverlaps)
+    BallCarRows bc;
+    bc.nv = bc.nf = bc.ns = 0;
+    for (int i = 0; i < count && i < 8; ++i) {
+        const BpProxy& pb = proxies[0];
+        const BpProxy& pc = proxies[i + 1];
+        CarState& car = A.cars[i];
+        const bool overlaps = i + 1 < body_count && pc.valid != 0 && !car.just_respawned &&
+                              !(pc.child_min.x > pb.child_max.x || pc.child_max.x < pb.child_min.x ||
+                                pc.child_min.y > pb.child_max.y || pc.child_max.y < pb.child_min.y ||
+                                pc.child_min.z > pb.child_max.z || pc.child_max.z < pb.child_min.z);
+        if (!overlaps) {
+            bcs[i].count = 0;
+            continue;
+        }
+        ball_car_contacts(bcs[i], b, car, A.cfgs[i], c, i, ext_delta, solver_vel_bt, sub_dt, bc);
+        if (!pre[i].is_demoed && !car.just_respawned)
+            commit_ball_hit_from_manifold(b, car, bcs[i], static_cast<uint32_t>(A.car_base + i + 1), env_tick,
+                                          hit_car_pos[i], hit_car_rot[i], hit_ball_pos, snap.car_start_vel[i],
+                                          snap.ball_start_vel);
+    }
+    // the ball's arena contacts (reference env_step.hpp:5219-5290): a sleeping ball a car touched is awake now,
+    // and looks at the arena when it still holds arena contact points
+    const bool awake_after = awake || bc.nv > 0 || bc.nf > 0 || bc.ns > 0;
     BallContactRows rows;
     rows.split_count = rows.vel_count = rows.fric_count = 0;
-    if (awake) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
+    if (awake_after && (awake || s.count != 0)) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
     // the cars' arena contacts, in slot order
     CarWorldRows cr;
     cr.nv = cr.nf = cr.ns = 0;
@@ -749,11 +900,11 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
         }
     }
     // velocity solve
-    if (rows.vel_count || rows.fric_count || cr.nv || cr.nf) {
+    if (rows.vel_count || rows.fric_count || cr.nv || cr.nf || bc.nv || bc.nf) {
         V3 dl{0, 0, 0}, da{0, 0, 0};
         V3 cdl[8], cda[8];
         for (int i = 0; i < count; ++i) cdl[i] = cda[i] = V3{0.0f, 0.0f, 0.0f};
-        unified_velocity_solve(rows, cr, list, n_list, dl, da, cdl, cda);
+        unified_velocity_solve(rows, bc, cr, list, n_list, dl, da, cdl, cda);
         ball_set_vel_bt(b, solver_vel_bt + dl);
         b.ang_vel = b.ang_vel + da;
         for (int i = 0; i < count; ++i) {
@@ -762,10 +913,10 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
         }
     }
     // position (split-impulse) solve
-    if (rows.split_count || cr.ns) {
+    if (rows.split_count || cr.ns || bc.ns) {
         V3 cpush[8], cturn[8];
         bool cbt[8];
-        const V3 push = unified_split_solve(rows, cr, list, n_list, cpush, cturn, cbt, count);
+        const V3 push = unified_split_solve(rows, bc, cr, list, n_list, cpush, cturn, cbt, count);
         if (!is_zero(push)) ball_set_pos_bt(b, b.pos_bt + push * sub_dt);
         for (int i = 0; i < count; ++i) {
             CarState& car = A.cars[i];
@@ -785,7 +936,7 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
     }
     // the ball's gravity, integration and deactivation clock
     if (!ball_sleeping) ball_set_vel_bt(b, b.vel_bt + uu_to_bt_div(ext_delta));
-    if (awake) {
+    if (awake_after) {
         ball_integrate(b, sub_dt);
         b.sleeping = 0;
         const bool below = len2(b.vel_bt) < kBallLinearSleepBt * kBallLinearSleepBt &&
@@ -795,9 +946,28 @@ RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, C
     for (int i = 0; i < count; ++i) car_world_finish(A.cars[i], pre[i], sub_dt);
 }
 
+// The game's extra ball-hit impulses of this tick, as a velocity change of the ball (reference ApplyBallExtraHits,
+// env_step.hpp:6929-6948).
+RG_HDI void apply_ball_extra_hits(BallState& b, CarState* cars, int count, const TickConfig& c) {
+    const float inv = 1.0f / c.ball_mass;
+    const float mass_bt = 1.0f / inv;
+    V3 v = b.vel_bt;
+    bool any = false;
+    for (int i = 0; i < count; ++i) {
+        BallHitInfo& h = cars[i].ball_hit_info;
+        if (!h.extra_pending) continue;
+        const V3 a = h.extra_hit_vel;
+        v = V3{v.x + ((a.x * 0.02f) * mass_bt) * inv, v.y + ((a.y * 0.02f) * mass_bt) * inv,
+               v.z + ((a.z * 0.02f) * mass_bt) * inv};
+        h.extra_pending = 0;
+        any = true;
+    }
+    if (any) ball_set_vel_bt(b, v);
+}
+
 // One tick of one arena with cars (reference StepEnvGeneric, env_step.hpp:7088-7180).
 RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
-                            const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
+                            BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
                             const PadLayout& pads_layout, bool report_fields) {
     const int count = A.count;
     update_game_visit_order(env, A.cars, count);
@@ -807,13 +977,15 @@ RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Br
     for (int k = 0; k < count; ++k) order[k] = car_visit_slot(env, k, count);
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
-        car_pre_tick(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i]);
+        const V3 start_vel = car_pre_tick(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i]);
         if (i < 8) {
+            snap.car_start_vel[i] = start_vel;
             snap.car_vel_bt[i] = A.cars[i].vel_bt;
             snap.car_ang_vel[i] = A.cars[i].ang_vel;
         }
     }
     ball_tick_start_quantize(b, c);
+    snap.ball_start_vel = b.vel;
     ball_clamp_and_drag(b, c);
     snap.ball_vel_bt = b.vel_bt;
     if (c.enable_boost_pads && count > 0 && A.pads)
@@ -823,7 +995,7 @@ RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Br
         vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh);
     }
     PreContactCar pre[8];
-    world_step_cars(b, s, bp, cws, c, mesh, A, pre, snap);
+    world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick);
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         CarState& car = A.cars[i];
@@ -840,6 +1012,7 @@ RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Br
         CarState& car = A.cars[order[k]];
         if (!car.is_demoed && car.driving_disabled) --car.driving_disabled;
     }
+    apply_ball_extra_hits(b, A.cars, count, c);
     env_tail(env, b, c, A.cars, count);
 }
 

@@ -102,3 +102,27 @@ class ControlStream:
             self.left[renew] = self.rng.integers(1, self.hold_max + 1, k)
         self.left -= 1
         return self.cur.copy()
+
+
+def chase_ball_controls(cars: np.ndarray, balls: np.ndarray, max_cars: int, rng: np.random.Generator,
+                        p_jump: float = 0.02) -> np.ndarray:
+    """A ball-chasing driver for every car slot (dense car rows [envs * max_cars, CAR_BYTES], balls [envs, BALL_BYTES]):
+    full throttle and boost, steering proportional to the heading error toward the arena's ball, rare jumps, seeded
+    air-control noise. The game's quaternions are (w, x, y, z); forward is the body x axis."""
+    n = cars.shape[0]
+    pos = cars[:, CAR_POS:CAR_POS + 12].copy().view(np.float32).astype(np.float64)
+    q = cars[:, CAR_ROT:CAR_ROT + 16].copy().view(np.float32).astype(np.float64)
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    yaw = np.arctan2(2.0 * (x * y + w * z), 1.0 - 2.0 * (y * y + z * z))
+    bpos = np.repeat(balls[:, OFF_POS:OFF_POS + 12].copy().view(np.float32).astype(np.float64), max_cars, axis=0)
+    want = np.arctan2(bpos[:, 1] - pos[:, 1], bpos[:, 0] - pos[:, 0])
+    err = (want - yaw + np.pi) % (2.0 * np.pi) - np.pi
+    ctrl = np.zeros((n, CONTROLS_BYTES), np.uint8)
+    f = np.zeros((n, 5), np.float32)
+    f[:, 0] = 1.0
+    f[:, 1] = np.clip(2.5 * err, -1.0, 1.0)
+    f[:, 2:5] = rng.uniform(-0.3, 0.3, (n, 3))
+    ctrl[:, :20] = f.view(np.uint8).reshape(n, 20)
+    ctrl[:, 20] = rng.random(n) < p_jump
+    ctrl[:, 21] = 1
+    return ctrl
