@@ -1,17 +1,21 @@
 """Throughput of the batched arena tick on B200 (arena-ticks/s), one JSON line on rank 0.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload mixed|balls]
 
-Workload: 16,384 ball-only arenas in the procedural ~11k-triangle arena, each ball started from a seeded position
-with a seeded velocity (uniform direction, speed up to 6000 uu/s); a step is one BatchSim step of 8 ticks (one
-kernel launch), as the reference's bench steps 8 ticks per call. Arenas are independent, so N GPUs run N shards of
-16,384 arenas each ("scaling": "weak") with no data-path collective; the only cross-rank traffic is the timing
-max-reduction.
+Workload `mixed` (default): 16,384 arenas per GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3 (seeded), default car body, in
+the procedural ~11k-triangle arena, started with reset_to_kickoff. Controls come from the seeded generator (throttle,
+steer, pitch, yaw, roll U[-1, 1]; jump / boost / handbrake Bernoulli 0.1 / 0.3 / 0.1; each sample held for U{1..30}
+ticks). A step is one BatchSim::step_with_device_controls of 8 ticks (one kernel launch) over a [8, car_capacity]
+control block resident in HBM. Workload `balls`: 16,384 ball-only arenas, balls at seeded positions with seeded
+velocities up to 6000 uu/s, 8 ticks per step.
+
+Arenas are independent, so N GPUs run N shards of 16,384 arenas each ("scaling": "weak") with no data-path collective;
+the only cross-rank traffic is the timing max-reduction.
 
 Timing: W untimed warm-up steps; then K steps, each timed with CUDA events on the launching stream after a 256 MiB L2
 flush (outside the events), barrier + synchronize around the timed region, max over ranks. `e2e` times the same steps
-through the C ABI from host code, including each step's device-to-host copy of every ball state (the observation) into
-pinned memory; BatchSim::step takes no per-step input, so h2d_bytes_per_step is 0.
+through the public API from host code: each step copies its control block from pinned host memory to the device and
+reads every car and ball state back into pinned memory (the observation), both inside the timed region.
 
 `--impl reference` times the reference's own CPU implementation (oracle/_ref, built from the reference's sources) on
 the same workload with all host threads, on a bounded sample of steps.
@@ -19,6 +23,7 @@ the same workload with all host threads, on a bounded sample of steps.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -33,12 +38,17 @@ sys.path.insert(0, ROOT)
 
 ENVS = 16384
 TICKS_PER_STEP = 8
+MAX_CARS = 6
 METRIC = "arena-ticks/s"
-WORKLOAD = "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step"
-# dram__bytes_read.sum + dram__bytes_write.sum of one tick_kernel launch at this workload, from the ncu capture
-# summarised in profiles/tick_kernel_ball_arenas_16k.md
-TRAFFIC_PER_LAUNCH = 16.01e6
-STATE_BYTES_PER_ARENA = 288 + 288 + 44  # ball struct + ball contact state + env struct, read and written per launch
+CAR_BYTES, BALL_BYTES, ENV_BYTES, WHEEL_BYTES, CAR_MANIFOLD_BYTES, CTRL_BYTES, PAD_BYTES = 880, 288, 44, 292, 208, 24, 16
+WORKLOADS = {
+    "mixed": "16384 arenas/GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3 from kickoff, seeded held controls, procedural "
+             "11k-tri arena, 8 ticks per launch",
+    "balls": "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step",
+}
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel at each workload, from the ncu
+# captures summarised under profiles/ (None: not captured)
+TRAFFIC_PER_LAUNCH = {"balls": 16.01e6, "mixed": None}
 
 
 def peaks():
@@ -127,35 +137,76 @@ def barrier(world):
         dist.barrier()
 
 
-def run_ours(args, world, rank, local):
-    import ctypes
+# ---- the mixed workload's inputs (shared by both arms) -----------------------------------------------------------
+def mixed_layout(seed: int):
+    """Cars per arena (2/4/6 with p = .55/.27/.18) and teams (the first half of an arena's cars blue, the rest
+    orange)."""
+    rng = np.random.default_rng(seed)
+    counts = rng.choice(np.array([2, 4, 6], np.int32), size=ENVS, p=[0.55, 0.27, 0.18]).astype(np.int32)
+    teams = np.zeros(ENVS * MAX_CARS, np.uint8)
+    for n in (2, 4, 6):
+        idx = np.nonzero(counts == n)[0]
+        for s in range(n // 2, n):
+            teams[idx * MAX_CARS + s] = 1
+    return counts, teams
 
+
+def control_blocks(n_steps: int, seed: int) -> np.ndarray:
+    """[n_steps, TICKS_PER_STEP, capacity, 24] control rows from the seeded generator (held U{1..30} ticks)."""
+    from tests import scenarios
+    cap = ENVS * MAX_CARS
+    stream = scenarios.ControlStream(cap, seed=seed, p_jump=0.1, hold_max=30)
+    out = np.empty((n_steps, TICKS_PER_STEP, cap, CTRL_BYTES), np.uint8)
+    for s in range(n_steps):
+        for t in range(TICKS_PER_STEP):
+            out[s, t] = stream.next()
+    return out
+
+
+def run_ours(args, world, rank, local):
     import torch
 
     from rocketgpu_b200 import abi, arena
     from rocketgpu_b200.batch_sim import BatchSim, SimConfig
-    from tests import scenarios
 
     torch.cuda.set_device(local)
     v, i = arena.generate()
-    sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=2), v, i, device=local)
-    sim.set_env_car_count(np.zeros(ENVS, np.int32))
-    default_ball = np.zeros(288, np.uint8)
-    abi.lib().rg_default_ball_state(default_ball.ctypes.data)
-    init = scenarios.ball_states(default_ball, ENVS, seed=1000 + rank)
-    sim.upload_ball_states(init)
+    lib = abi.lib()
     stream = torch.cuda.current_stream()
     s_handle = ctypes.c_void_p(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    lib = abi.lib()
+    mixed = args.workload == "mixed"
+    n_steps = args.warmup + args.steps
+    if mixed:
+        sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=MAX_CARS, kickoff_settled=0), v, i, device=local)
+        counts, teams = mixed_layout(seed=7 + rank)
+        sim.set_env_car_count(counts)
+        sim.set_teams(teams)
+        sim.reset_to_kickoff(1000 + rank)
+        cap = sim.car_capacity()
+        blocks_host = control_blocks(n_steps, seed=2000 + rank)
+        blocks_dev = torch.from_numpy(blocks_host.reshape(n_steps, -1)).to("cuda")
+        cars_total = int(counts.sum())
+    else:
+        from tests import scenarios
+        sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=2), v, i, device=local)
+        sim.set_env_car_count(np.zeros(ENVS, np.int32))
+        default_ball = np.zeros(BALL_BYTES, np.uint8)
+        lib.rg_default_ball_state(default_ball.ctypes.data)
+        sim.upload_ball_states(scenarios.ball_states(default_ball, ENVS, seed=1000 + rank))
+        cap, cars_total = 0, 0
 
-    def step():
-        rc = lib.rg_batch_step(sim._h, TICKS_PER_STEP, s_handle)
+    def step(k, ctrl_ptr=None):
+        if mixed:
+            ptr = ctrl_ptr if ctrl_ptr is not None else blocks_dev[k].data_ptr()
+            rc = lib.rg_batch_step_with_device_controls(sim._h, ctypes.c_void_p(ptr), TICKS_PER_STEP, cap, s_handle)
+        else:
+            rc = lib.rg_batch_step(sim._h, TICKS_PER_STEP, s_handle)
         if rc != 0:
             raise RuntimeError(lib.rg_last_error().decode())
 
-    for _ in range(args.warmup):
-        step()
+    for k in range(args.warmup):
+        step(k)
     torch.cuda.synchronize()
     # device-timed region
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -165,7 +216,7 @@ def run_ours(args, world, rank, local):
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
-            step()
+            step(args.warmup + k)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
     barrier(world)
@@ -174,43 +225,70 @@ def run_ours(args, world, rank, local):
     arena_ticks = ENVS * TICKS_PER_STEP * args.steps * world
     value = arena_ticks / dev_s
 
-    # end to end through the C ABI: step + D2H of all ball states into pinned memory, host wall time per step
-    pinned = torch.empty((ENVS, 288), dtype=torch.uint8, pin_memory=True)
+    # end to end through the public API: per step, the H2D copy of the step's control block from pinned memory, the
+    # step, and the D2H read of every car and ball state into pinned memory; host wall time
+    ball_pin = torch.empty((ENVS, BALL_BYTES), dtype=torch.uint8, pin_memory=True)
+    h2d = 0
+    if mixed:
+        car_pin = torch.empty((cap, CAR_BYTES), dtype=torch.uint8, pin_memory=True)
+        ctrl_pin = torch.from_numpy(blocks_host[args.warmup:].reshape(args.steps, -1)).pin_memory()
+        ctrl_dev = torch.empty(ctrl_pin.shape[1], dtype=torch.uint8, device="cuda")
+        h2d = ctrl_pin.shape[1]
+        # the e2e pass replays the same control blocks from the state the timed pass left: same work per step
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-        rc = lib.rg_batch_download_ball_states(sim._h, ctypes.c_void_p(pinned.data_ptr()), ENVS, s_handle)
+    for k in range(args.steps):
+        if mixed:
+            ctrl_dev.copy_(ctrl_pin[k], non_blocking=True)
+            step(None, ctrl_dev.data_ptr())
+            rc = lib.rg_batch_download_car_states(sim._h, ctypes.c_void_p(car_pin.data_ptr()), cap, s_handle)
+            if rc != 0:
+                raise RuntimeError(lib.rg_last_error().decode())
+        else:
+            step(k)
+        rc = lib.rg_batch_download_ball_states(sim._h, ctypes.c_void_p(ball_pin.data_ptr()), ENVS, s_handle)
         if rc != 0:
             raise RuntimeError(lib.rg_last_error().decode())
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = arena_ticks / e2e_s
+    d2h = ENVS * BALL_BYTES + cap * CAR_BYTES
 
     hbm, peak_kind = peaks()
     per_launch_ms = float(np.mean(launch_ms))
-    bytes_per_launch = 2 * STATE_BYTES_PER_ARENA * ENVS
+    if mixed:
+        # algorithmic state bytes of one launch: each arena's ball, ball contact state, env, broadphase history and
+        # pads read and written once; each active car's state, wheel record and car-mesh manifold read and written
+        # once per tick, its controls read once per tick
+        per_arena = 2 * (BALL_BYTES + 288 + ENV_BYTES + 1104 + 34 * PAD_BYTES)
+        per_car_tick = 2 * (CAR_BYTES + WHEEL_BYTES + CAR_MANIFOLD_BYTES) + CTRL_BYTES
+        bytes_per_launch = ENVS * per_arena + cars_total * per_car_tick * TICKS_PER_STEP
+    else:
+        bytes_per_launch = 2 * (BALL_BYTES + 288 + ENV_BYTES) * ENVS
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ball states)",
-        "config": {"workload": WORKLOAD, "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
-                   "l2": "256 MiB flush before every timed step", "parallelism": f"arena shards x{world}"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded kickoff arenas and controls)" if mixed else "synthetic (seeded ball states)",
+        "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
+                   "cars_per_gpu": cars_total, "l2": "256 MiB flush before every timed step",
+                   "parallelism": f"arena shards x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_kind, "traffic": TRAFFIC_PER_LAUNCH,
-                     "note": "state traffic only; the tick is FP32-issue/latency bound, not HBM bound"},
-        "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ENVS * 288},
+                     "peak_source": peak_kind, "traffic": TRAFFIC_PER_LAUNCH[args.workload],
+                     "note": "algorithmic state bytes per launch / launch time; the tick is FP32-issue / latency "
+                             "bound (data-dependent branches, dependent loads), not HBM bound"},
+        "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sample_steps=args.cpu_steps)
+        line["cpu_baseline"] = cpu_baseline(args.workload, sample_steps=args.cpu_steps)
     return line
 
 
-def cpu_baseline(sample_steps: int = 4):
+def cpu_baseline(workload: str, sample_steps: int = 60):
     """The reference's own CPU BatchSim (oracle/_ref) on the same workload, all host threads, a bounded sample."""
     from rocketgpu_b200 import arena
     from tests import oracle_ref, scenarios
@@ -220,29 +298,46 @@ def cpu_baseline(sample_steps: int = 4):
     cores = os.cpu_count() or 1
     os.environ["ROCKETGPU_CPU_THREADS"] = str(cores)
     v, i = arena.generate()
-    sim = oracle_ref.OracleSim(ENVS, 2, v, i, kickoff_settled=False)
-    sim.set_env_car_count([0] * ENVS)
-    _, default_ball, _, _, _ = oracle_ref.default_states()
-    sim.upload_balls(scenarios.ball_states(default_ball, ENVS, seed=1000))
-    sim.step(TICKS_PER_STEP)
+    if workload == "mixed":
+        sim = oracle_ref.OracleSim(ENVS, MAX_CARS, v, i, kickoff_settled=False)
+        counts, teams = mixed_layout(seed=7)
+        sim.set_env_car_count(counts)
+        sim.set_teams(teams)
+        sim.reset_to_kickoff(1000)
+        cap = ENVS * MAX_CARS
+        stream = scenarios.ControlStream(cap, seed=2000, p_jump=0.1, hold_max=30)
+
+        def one(k):
+            block = np.stack([stream.next() for _ in range(TICKS_PER_STEP)])
+            sim.step_with_controls(block.reshape(-1, CTRL_BYTES), TICKS_PER_STEP, cap)
+    else:
+        sim = oracle_ref.OracleSim(ENVS, 2, v, i, kickoff_settled=False)
+        sim.set_env_car_count([0] * ENVS)
+        _, default_ball, _, _, _ = oracle_ref.default_states()
+        sim.upload_balls(scenarios.ball_states(default_ball, ENVS, seed=1000))
+
+        def one(k):
+            sim.step(TICKS_PER_STEP)
+    one(0)
     t0 = time.perf_counter()
-    for _ in range(sample_steps):
-        sim.step(TICKS_PER_STEP)
+    for k in range(sample_steps):
+        one(k + 1)
     dt = time.perf_counter() - t0
     return {"value": ENVS * TICKS_PER_STEP * sample_steps / dt, "unit": "arena-ticks/s", "cores": cores,
             "kind": "reference",
-            "sample": f"{sample_steps} steps x {TICKS_PER_STEP} ticks x {ENVS} arenas, ROCKETGPU_CPU_THREADS={cores}"}
+            "sample": f"{sample_steps} steps x {TICKS_PER_STEP} ticks x {ENVS} arenas ({workload}), "
+                      f"ROCKETGPU_CPU_THREADS={cores}"}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return None
-    cb = cpu_baseline(sample_steps=max(1, args.steps))
+    cb = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, args.cpu_steps)))
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "arena-ticks/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ball states)",
-        "config": {"workload": WORKLOAD, "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded kickoff arenas and controls)",
+        "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP},
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -255,7 +350,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -415,7 +415,7 @@ RG_HDI void ball_car_point_rows(BallCarRows& rows, const BallState& b, const Car
 
 // The car's contact with the ball this tick: fresh geometry merged into the retained manifold, rows per point
 // (reference AppendBallCarContactRowsRetained).
-RG_HDI void ball_car_contacts(BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
+RG_NOINL void ball_car_contacts(BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
                               const TickConfig& tc, int car, V3 ball_ext_uu, V3 ball_lin_bt, float dt,
                               BallCarRows& rows) {
     const float thr = ball_car_threshold_bt(cfg, tc.ball_radius);

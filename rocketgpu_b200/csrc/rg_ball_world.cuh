@@ -720,7 +720,7 @@ RG_HDI bool ball_predictive_hit(const BallState& b, const MeshDevice& m, float d
 // Builds the ball's mesh manifold and its contact rows for this tick (the mesh branch of
 // AppendBallWorldSpecialContactRows). `solver_vel_bt` is the ball's linear velocity the solver starts from;
 // `ext_delta` the external (gravity) velocity change in uu/s.
-RG_HDI void ball_mesh_contacts(const BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& m,
+RG_NOINL void ball_mesh_contacts(const BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& m,
                                V3 ext_delta, V3 solver_vel_bt, float dt, BallContactRows& rows) {
     const float radius_bt = c.ball_radius * (1.0f / 50.0f);
     const float threshold = (radius_bt + 0.08f) * 0.02f;

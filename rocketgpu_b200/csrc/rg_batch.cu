@@ -7,6 +7,7 @@
 // 148 SMs. Ticks per launch amortise the state load/store and launch latency.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -89,12 +90,20 @@ struct rg_batch {
     DeviceArray<rg::Broadphase> broadphase;    // per arena: sweep history and manifold list
     DeviceArray<rg::CarWorldScratch> car_world;  // per car slot: the car/mesh manifold
     DeviceArray<rg::BallCarScratch> ball_car;     // per car slot: the car/ball manifold
+    DeviceArray<rg::CarTickRecord> car_records;  // per car slot: this tick's record of the car's own update
+    DeviceArray<rg::ArenaTickSnap> arena_snaps;  // per arena: the ball's velocities at this tick's start
+    // Step order: arenas sorted by car count (so a warp's arenas take the same loops), and the active car slots of
+    // those arenas in that order (one thread each in the per-car kernel). Rebuilt by set_env_car_count.
+    DeviceArray<int32_t> arena_order;
+    DeviceArray<int32_t> active_cars;
+    int32_t active_car_count = 0;
     rg::PadLayout pad_layout{};
     // Pads stay at their initial state until a car exists or pads are uploaded; until then ball-only arenas skip them.
     bool pads_live = false;
     rg::MeshHost mesh_host;
     rg::MeshDevice mesh;
     std::vector<int32_t> host_car_count;
+    std::vector<int32_t> host_arena_order, host_active_cars;
     int launch_threads = 32;
 };
 
@@ -197,36 +206,71 @@ struct CarTickArgs {
     rg::Broadphase* broadphase;
     rg::CarWorldScratch* car_world;
     rg::BallCarScratch* ball_car;
+    rg::CarTickRecord* records;
+    rg::ArenaTickSnap* snaps;
+    const int32_t* arena_order;
+    const int32_t* active_cars;
+    int32_t active_car_count;
 };
 
-// Arenas with cars: ball, env and manifold scratch in registers as in tick_kernel; cars, wheel records and pads are
-// edited in place in global memory (L1-cached).
-__global__ void __launch_bounds__(32) car_tick_kernel(CarTickArgs a, int ticks) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.base.env_count) return;
-    rg::BallState b = a.base.balls[e];
-    rg::EnvState env = a.base.envs[e];
-    rg::BallWorldScratch s = a.base.ball_world[e];
+__device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e, int t) {
     const int car_base = e * a.max_cars;
     rg::ArenaCars A;
     A.cars = a.cars + car_base;
     A.wheels = a.wheels + car_base;
     A.cfgs = a.car_cfgs + car_base;
     A.pads = a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr;
+    A.controls = a.controls ? a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base
+                            : nullptr;
     A.count = a.base.env_car_count[e];
     A.max_cars = a.max_cars;
     A.car_base = car_base;
-    for (int t = 0; t < ticks; ++t) {
-        A.controls = a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base;
-        rg::arena_tick_cars(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc, a.base.mesh, A,
-                            a.pad_layout, t + 1 == ticks);
-    }
+    return A;
+}
+
+// Tick part 1, one thread per arena in step order: vehicle order, the ball's tick start, pad timers.
+__global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.base.env_count) return;
+    const int e = a.arena_order[k];
+    rg::BallState b = a.base.balls[e];
+    rg::EnvState env = a.base.envs[e];
+    rg::arena_tick_begin(env, b, arena_cars(a, e, t), a.base.tc, a.pad_layout, a.snaps[e]);
+    a.base.balls[e] = b;
+    a.base.envs[e] = env;
+}
+
+// Tick part 2, one thread per active car: the car's tick start and vehicle update (four suspension rays against the
+// arena mesh and the ball, tyres, jumps, boost, air control). The ball is only read.
+__global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.active_car_count) return;
+    const int idx = a.active_cars[k];
+    const int e = idx / a.max_cars;
+    const rg::CarControls& ctrl =
+        a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+    rg::car_tick_vehicle(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], a.base.mesh,
+                         a.records[idx]);
+}
+
+// Tick part 3, one thread per arena in step order: wheel pushes on the ball, the world step, post-tick, pads, goal.
+__global__ void __launch_bounds__(32) arena_finish_kernel(CarTickArgs a, int t, int report_fields) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.base.env_count) return;
+    const int e = a.arena_order[k];
+    rg::BallState b = a.base.balls[e];
+    rg::EnvState env = a.base.envs[e];
+    rg::BallWorldScratch s = a.base.ball_world[e];
+    const int car_base = e * a.max_cars;
+    rg::arena_tick_finish(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc,
+                          a.base.mesh, arena_cars(a, e, t), a.pad_layout, report_fields != 0, a.records + car_base,
+                          a.snaps[e]);
     a.base.balls[e] = b;
     a.base.envs[e] = env;
     a.base.ball_world[e] = s;
 }
 
-void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s) {
+CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stride) {
     CarTickArgs a;
     a.base.balls = b->balls.ptr;
     a.base.envs = b->envs.ptr;
@@ -246,10 +290,27 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     a.broadphase = b->broadphase.ptr;
     a.car_world = b->car_world.ptr;
     a.ball_car = b->ball_car.ptr;
+    a.records = b->car_records.ptr;
+    a.snaps = b->arena_snaps.ptr;
+    a.arena_order = b->arena_order.ptr;
+    a.active_cars = b->active_cars.ptr;
+    a.active_car_count = b->active_car_count;
+    return a;
+}
+
+// Arenas with cars: three launches per tick (arena begin, per-car vehicle update, arena finish).
+void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s) {
+    if (b->env_count == 0) return;
+    const CarTickArgs a = car_tick_args(b, controls, stride);
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
-    car_tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
-    check(cudaGetLastError(), "car_tick_kernel launch");
+    const int car_blocks = (b->active_car_count + 63) / 64;
+    for (int t = 0; t < ticks; ++t) {
+        arena_begin_kernel<<<blocks, threads, 0, s>>>(a, t);
+        if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s>>>(a, t);
+        arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, t + 1 == ticks ? 1 : 0);
+    }
+    check(cudaGetLastError(), "car tick launch");
 }
 
 // reset_to_kickoff for every arena (reference BatchSim::reset_to_kickoff, src/rocketgpu.cpp:2085-2132).
@@ -271,25 +332,8 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
 }
 
 void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
-    CarTickArgs a;
-    a.base.balls = b->balls.ptr;
-    a.base.envs = b->envs.ptr;
-    a.base.env_car_count = b->env_car_count.ptr;
-    a.base.ball_world = b->ball_world.ptr;
-    a.base.env_count = b->env_count;
-    a.base.tc = b->tc;
-    a.base.mesh = b->mesh;
-    a.cars = b->cars.ptr;
-    a.wheels = b->wheels.ptr;
-    a.car_cfgs = b->car_cfgs.ptr;
+    CarTickArgs a = car_tick_args(b, nullptr, 0);
     a.pads = b->pads.ptr;
-    a.controls = nullptr;
-    a.control_stride = 0;
-    a.max_cars = b->max_cars;
-    a.pad_layout = b->pad_layout;
-    a.broadphase = b->broadphase.ptr;
-    a.car_world = b->car_world.ptr;
-    a.ball_car = b->ball_car.ptr;
     reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed);
     check(cudaGetLastError(), "reset_kickoff_kernel launch");
 }
@@ -309,6 +353,30 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
     const int blocks = (b->env_count + threads - 1) / threads;
     tick_kernel<<<blocks, threads, 0, s>>>(a, ticks);
     check(cudaGetLastError(), "tick_kernel launch");
+}
+
+// The step order (reference set_env_car_count rebuilds its step order, src/rocketgpu.cpp:2920-2932): arenas stably
+// sorted by car count, and the active car slots of those arenas in that order. The host copies stay in the batch
+// until the caller's stream has finished the upload (set_env_car_count synchronises it).
+void rebuild_step_order(rg_batch* b, cudaStream_t s) {
+    std::vector<int32_t>& order = b->host_arena_order;
+    order.resize(b->env_count);
+    for (int32_t e = 0; e < b->env_count; ++e) order[e] = e;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return b->host_car_count[x] < b->host_car_count[y]; });
+    std::vector<int32_t>& cars = b->host_active_cars;
+    cars.clear();
+    for (int32_t e : order)
+        for (int32_t i = 0; i < b->host_car_count[e]; ++i) cars.push_back(e * b->max_cars + i);
+    if (b->env_count)
+        check(cudaMemcpyAsync(b->arena_order.ptr, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              s),
+              "step order");
+    if (!cars.empty())
+        check(cudaMemcpyAsync(b->active_cars.ptr, cars.data(), cars.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              s),
+              "active cars");
+    b->active_car_count = static_cast<int32_t>(cars.size());
 }
 
 rg::TickConfig resolve_tick_config(const rg_sim_config& c) {
@@ -505,6 +573,11 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         if (cap) check(cudaMemset(b->car_world.ptr, 0, cap * sizeof(rg::CarWorldScratch)), "car manifolds");
         b->ball_car.alloc(cap);
         if (cap) check(cudaMemset(b->ball_car.ptr, 0, cap * sizeof(rg::BallCarScratch)), "car-ball manifolds");
+        b->car_records.alloc(cap);
+        b->arena_snaps.alloc(b->env_count);
+        b->arena_order.alloc(b->env_count);
+        b->active_cars.alloc(cap);
+        rebuild_step_order(b.get(), nullptr);
         if (cap) {
             rg_car_state c0;
             rg_default_car_state(&c0);
@@ -566,6 +639,7 @@ RG_API int rg_batch_set_env_car_count(rg_batch* b, const int32_t* counts, size_t
         DeviceGuard dg(b->device);
         std::memcpy(b->host_car_count.data(), counts, count * sizeof(int32_t));
         for (size_t i = 0; i < count; ++i) b->pads_live = b->pads_live || counts[i] > 0;
+        rebuild_step_order(b, static_cast<cudaStream_t>(stream));
         check(cudaMemcpyAsync(b->env_car_count.ptr, counts, count * sizeof(int32_t), cudaMemcpyHostToDevice,
                               static_cast<cudaStream_t>(stream)),
               "set_env_car_count");

@@ -484,7 +484,7 @@ struct BpEntry {
 // `mesh_max`: the arena mesh's bounds (Bullet units); `pred_mask`: bodies with a predictive contact this tick;
 // `ball_static_skipped`: the ball sleeps, so its static pairs make no new manifold. Fills `out` (sorted) and returns
 // its length.
-RG_HDI int bp_build_manifold_list(Broadphase& h, const BpProxy* proxies, int body_count, V3 mesh_min, V3 mesh_max,
+RG_NOINL int bp_build_manifold_list(Broadphase& h, const BpProxy* proxies, int body_count, V3 mesh_min, V3 mesh_max,
                                   uint32_t pred_mask, bool ball_static_skipped, BpEntry* out) {
     Sweep s{h, body_count};
     const bool fresh = h.handle_count == 0;

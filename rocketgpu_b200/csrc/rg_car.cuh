@@ -847,7 +847,7 @@ RG_HDI void apply_auto_flip(CarState& c, const CarConfig& cfg, const TickConfig&
 
 // Everything the tick does to a car before the vehicle update (reference PreTickCarPrePhysics, env_step.hpp:2981-3113),
 // for a car that always has a wheel record.
-RG_HDI void car_pre_physics(CarState& c, CarControls k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w,
+RG_NOINL void car_pre_physics(CarState& c, CarControls k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w,
                             Q4 snap_rot, V3 snap_vel_uu) {
     const float dt = tc.tick_dt;
     c.cal_pre_flags = 0;

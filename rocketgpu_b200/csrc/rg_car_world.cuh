@@ -350,7 +350,7 @@ struct CarWorldContactResult {
 // The car's contacts with the arena mesh for this tick: refresh the retained manifold, collect candidates from the
 // triangles the box overlaps, merge them into the manifold and emit rows (body index `body`, source tag 100).
 // `listed`: the car/mesh manifold exists in the broadphase list.
-RG_HDI CarWorldContactResult car_mesh_contacts(CarState& c, const CarConfig& cfg, CarWorldScratch& ws, bool listed,
+RG_NOINL CarWorldContactResult car_mesh_contacts(CarState& c, const CarConfig& cfg, CarWorldScratch& ws, bool listed,
                                                const MeshDevice& mesh, const TickConfig& tc, int body,
                                                CarWorldRows& rows) {
     CarWorldContactResult res;

@@ -752,7 +752,7 @@ struct Results {
 };
 
 // btGjkEpaSolver2::Penetration (with margins).
-RG_HDI bool penetration(const Shape& s0, const Xform& w0, const Shape& s1, const Xform& w1, V3 guess, Results& r) {
+RG_NOINL bool penetration(const Shape& s0, const Xform& w0, const Shape& s1, const Xform& w1, V3 guess, Results& r) {
     r.witness0 = r.witness1 = V3{0.0f, 0.0f, 0.0f};
     Gjk g;
     g.shape = make_minkowski(s0, w0, s1, w1, true);
@@ -780,7 +780,7 @@ RG_HDI bool penetration(const Shape& s0, const Xform& w0, const Shape& s1, const
     return true;
 }
 // btGjkEpaSolver2::Distance (no margins). Returns false when the shapes overlap or GJK fails.
-RG_HDI bool distance(const Shape& s0, const Xform& w0, const Shape& s1, const Xform& w1, V3 guess, Results& r) {
+RG_NOINL bool distance(const Shape& s0, const Xform& w0, const Shape& s1, const Xform& w1, V3 guess, Results& r) {
     r.witness0 = r.witness1 = V3{0.0f, 0.0f, 0.0f};
     Gjk g;
     g.shape = make_minkowski(s0, w0, s1, w1, false);
@@ -1086,7 +1086,7 @@ RG_HDI Xform basis_xform(V3 f, V3 r, V3 u, V3 origin) {
 // (reference RunCarArenaTriangleGjkSimplex / RunBallCarGjkSimplex, triangle_and_carcar.hpp:206-300, 538-624):
 // iterates the Voronoi simplex toward the origin until a termination rule fires. Returns whether it ended on a rule
 // that yields closest points (`pa`, `pb`, world space); `degenerate` records which rule.
-RG_HDI bool pair_detector(const Shape& a, const Xform& xa, const Shape& b, const Xform& xb, float max_dist_sq,
+RG_NOINL bool pair_detector(const Shape& a, const Xform& xa, const Shape& b, const Xform& xb, float max_dist_sq,
                           V3& cached_axis, int& degenerate, float& squared_distance, V3& pa, V3& pb) {
     constexpr float kRelError2 = 1.0e-6f;
     bool check_simplex = false;
@@ -1156,7 +1156,7 @@ RG_HDI bool pair_detector(const Shape& a, const Xform& xa, const Shape& b, const
 // Closest points / penetration of the car's hitbox (half extents `raw_half_bt`, Bullet margin 0.04) and a triangle
 // (reference ComputeCarArenaTriangleContact). Returns false when there is no contact within 10 bt; otherwise the
 // signed distance and the witness point on the triangle.
-RG_HDI bool box_triangle_contact(V3 basis_f, V3 basis_r, V3 basis_u, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt,
+RG_NOINL bool box_triangle_contact(V3 basis_f, V3 basis_r, V3 basis_u, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt,
                                  V3 ta, V3 tb, V3 tc, float& out_distance_bt, V3& out_point_on_b_bt) {
     const Shape box = make_box(raw_half_bt, 0.04f);
     const Shape tri = make_triangle(ta, tb, tc);
@@ -1273,7 +1273,7 @@ struct BallBoxContact {
 // The car's hitbox (raw half extents, Bullet margin 0.04) against the ball's sphere (reference
 // ComputeBallCarContactGeometryGjk, triangle_and_carcar.hpp:626-821): the GJK pair detector, EPA when they overlap,
 // the contact kept within the breaking threshold. False leaves the caller to the sphere-box fallback.
-RG_HDI bool ball_box_contact(V3 cf, V3 cr, V3 cu, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt, V3 bx, V3 by,
+RG_NOINL bool ball_box_contact(V3 cf, V3 cr, V3 cu, V3 car_pos_bt, V3 child_offset_bt, V3 raw_half_bt, V3 bx, V3 by,
                              V3 bz, V3 ball_pos_bt, float radius_bt, float threshold_bt, BallBoxContact& out) {
     const Shape box = make_box(raw_half_bt, 0.04f);
     const Shape sphere = make_sphere(radius_bt);

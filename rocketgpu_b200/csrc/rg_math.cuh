@@ -13,9 +13,13 @@
 #if defined(__CUDACC__)
 #define RG_HD __host__ __device__ __forceinline__
 #define RG_HDI __host__ __device__ inline
+// Large phase functions stay out of line so their stack frames share one region instead of each holding its own
+// slice of the caller's frame: the tick touches fewer distinct local-memory lines per thread.
+#define RG_NOINL static __host__ __device__ __noinline__
 #else
 #define RG_HD inline
 #define RG_HDI inline
+#define RG_NOINL static inline
 #endif
 
 namespace rg {

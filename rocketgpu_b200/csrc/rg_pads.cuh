@@ -231,7 +231,7 @@ RG_HDI void pad_sweep_touch_steps(CarState* cars, int car_base, int max_cars, in
 
 // The pads' part of the tick tail (reference BoostPadTouchPassForEnv, :2706-2835, and PostTickBoostPadsForEnv,
 // :2851-2892). `order` lists the car slots in visit order.
-RG_HDI void pads_tail(CarState* cars, int car_base, int max_cars, const CarConfig* cfgs, int count, const int* order,
+RG_NOINL void pads_tail(CarState* cars, int car_base, int max_cars, const CarConfig* cfgs, int count, const int* order,
                       PadState* pads, const PadLayout& L, const TickConfig& tc) {
     if (!tc.enable_boost_pads || tc.frame_frac < 0.0f) return;
     for (int k = 0; k < count; ++k) {

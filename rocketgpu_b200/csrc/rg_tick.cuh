@@ -377,7 +377,7 @@ RG_HDI bool car_predictive_hit(const CarState& c, const CarConfig& cfg, const Me
 // Rows act on their bodies' velocity deltas (a car-ball row on both, reference
 // SolveBallVelocity{Normal,Friction}RowWithAccumulators, arena_geometry.hpp:2618-2750); one iteration count (stop
 // when nothing changed) covers all.
-RG_HDI void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list,
+RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list,
                                    int n_list, V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
     constexpr int kMax = kMaxBallVelRows + kMaxBallCarRows + kMaxCarWorldRows;
     uint8_t nb[kMax], ni[kMax], fb[kMax], fi[kMax];
@@ -615,7 +615,7 @@ RG_HDI void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorl
 // SolveUnifiedBallSplitRow, :3523-3600). Returns the ball's push velocity; the cars' push and turn velocities come
 // back in `car_push` / `car_turn`, `car_bt` telling which cars had Bullet-unit rows (every row here carries Bullet
 // units, so a car is in Bullet units when any of its arena or car-ball rows exists, MarkBtSplitAccumulators).
-RG_HDI V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list, int n_list,
+RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list, int n_list,
                               V3* car_push, V3* car_turn, bool* car_bt, int count) {
     constexpr int kMax = kMaxBallSplitRows + kMaxBallCarRows + kMaxCarWorldRows;
     for (int i = 0; i < count; ++i) car_bt[i] = false;
@@ -760,7 +760,7 @@ RG_HDI V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows
 // unified velocity and position solves, then integration; car-ball contacts (reference env_step.hpp:5045-5133)
 // with their ball-hit bookkeeping. Car/car contacts are not built yet: two cars whose boxes meet only shape the
 // manifold list here.
-RG_HDI void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
+RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                             BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
                             PreContactCar* pre, const TickSnap& snap, uint64_t env_tick) {
     const int count = A.count;
@@ -965,35 +965,64 @@ RG_HDI void apply_ball_extra_hits(BallState& b, CarState* cars, int count, const
     if (any) ball_set_vel_bt(b, v);
 }
 
-// One tick of one arena with cars (reference StepEnvGeneric, env_step.hpp:7088-7180).
-RG_HDI void arena_tick_cars(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
-                            BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
-                            const PadLayout& pads_layout, bool report_fields) {
+// A tick of an arena with cars runs in three parts, so that the cars' own updates can run one thread per car:
+//   arena_tick_begin   (per arena)  the game's vehicle order, the ball's tick start, the pads' timers;
+//   car_tick_vehicle   (per car)    the car's tick start and its vehicle update (suspension rays, tyres, jumps,
+//                                   boost, air control), recording what the world step needs from it;
+//   arena_tick_finish  (per arena)  the wheel pushes on the ball in car order, the world step, post-tick, pads, goal.
+// Reordering is exact: a car's tick start and vehicle update read and write only that car (the ball only through its
+// position, which none of them moves), and the ball's tick start reads no car, so running the cars' parts after the
+// ball's tick start and before any push is applied gives the reference's results bit for bit
+// (reference StepEnvGeneric, env_step.hpp:7088-7180).
+
+// What the world step needs from one car's tick start and vehicle update.
+struct CarTickRecord {
+    V3 start_vel;  // uu velocity right after the tick-start quantisation (ball-hit impulse)
+    V3 vel_bt, ang_vel;  // velocities the broadphase predicts motion with
+    WheelBallPushes pushes;
+};
+// The ball's velocities at the tick start.
+struct ArenaTickSnap {
+    V3 ball_start_vel, ball_vel_bt;
+};
+
+RG_HDI void arena_tick_begin(EnvState& env, BallState& b, const ArenaCars& A, const TickConfig& c,
+                             const PadLayout& pads_layout, ArenaTickSnap& as) {
     const int count = A.count;
     update_game_visit_order(env, A.cars, count);
     env.goal_scored_this_tick = 0;
+    ball_tick_start_quantize(b, c);
+    as.ball_start_vel = b.vel;
+    ball_clamp_and_drag(b, c);
+    as.ball_vel_bt = b.vel_bt;
+    if (c.enable_boost_pads && count > 0 && A.pads)
+        for (int p = 0; p < pads_layout.count; ++p) pad_pre_tick(A.pads[p], c.tick_dt);
+}
+
+RG_HDI void car_tick_vehicle(CarState& car, const CarControls& k, const CarConfig& cfg, const TickConfig& c,
+                             WheelRuntime& w, const BallState& b, const MeshDevice& mesh, CarTickRecord& r) {
+    r.start_vel = car_pre_tick(car, k, cfg, c, w);
+    r.vel_bt = car.vel_bt;
+    r.ang_vel = car.ang_vel;
+    vehicle_update(car, k, cfg, c, w, b, mesh, r.pushes);
+}
+
+RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
+                              BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
+                              const PadLayout& pads_layout, bool report_fields, const CarTickRecord* recs,
+                              const ArenaTickSnap& as) {
+    const int count = A.count;
     int order[8];
     TickSnap snap;
     for (int k = 0; k < count; ++k) order[k] = car_visit_slot(env, k, count);
-    for (int k = 0; k < count; ++k) {
-        const int i = order[k];
-        const V3 start_vel = car_pre_tick(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i]);
-        if (i < 8) {
-            snap.car_start_vel[i] = start_vel;
-            snap.car_vel_bt[i] = A.cars[i].vel_bt;
-            snap.car_ang_vel[i] = A.cars[i].ang_vel;
-        }
+    for (int i = 0; i < count && i < 8; ++i) {
+        snap.car_start_vel[i] = recs[i].start_vel;
+        snap.car_vel_bt[i] = recs[i].vel_bt;
+        snap.car_ang_vel[i] = recs[i].ang_vel;
     }
-    ball_tick_start_quantize(b, c);
-    snap.ball_start_vel = b.vel;
-    ball_clamp_and_drag(b, c);
-    snap.ball_vel_bt = b.vel_bt;
-    if (c.enable_boost_pads && count > 0 && A.pads)
-        for (int p = 0; p < pads_layout.count; ++p) pad_pre_tick(A.pads[p], c.tick_dt);
-    for (int k = 0; k < count; ++k) {
-        const int i = order[k];
-        vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh);
-    }
+    snap.ball_start_vel = as.ball_start_vel;
+    snap.ball_vel_bt = as.ball_vel_bt;
+    for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
     world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick);
     for (int k = 0; k < count; ++k) {

@@ -150,7 +150,7 @@ RG_HDI void wheel_ray_velocity_terms(const CarState& c, V3 car_up, V3 hit_point_
 // Closest mesh hit of a segment, rejecting hits nearer than sqrt(min_fraction_sq) of it; returns the hit fraction,
 // the triangle and the source's signed plane distance (reference HostRayCastArenaMeshBlocks,
 // host_validation_and_contact_debug.hpp:1603-1672, as CastArenaRayDeltaBt runs it).
-RG_HDI bool mesh_ray_cast(const MeshDevice& m, V3 from, V3 to, float min_fraction_sq, float& out_fraction,
+RG_NOINL bool mesh_ray_cast(const MeshDevice& m, V3 from, V3 to, float min_fraction_sq, float& out_fraction,
                           const DevTri*& out_tri, float& out_dist_a) {
     bool hit = false;
     float hit_fraction = 0.0f, win_dist_a = 0.0f;
@@ -717,8 +717,28 @@ RG_HDI void apply_boost(CarState& c, const CarControls& k, const TickConfig& tc,
 // ---- the vehicle update -------------------------------------------------------------------------------------------
 // reference PreTickCar (env_step.hpp:3115-3484) with PreTickVehicleDynamics (raycast_wheels_and_contact_prep.hpp:
 // 2618-2953), WheelRayPhase (:2074-2238) and CombineWheelContacts (:2240-2282).
-RG_HDI void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg, const TickConfig& tc,
-                           WheelRuntime& wr, BallState& ball, const MeshDevice& mesh) {
+// Wheel rays that landed on the ball this tick, in the car's wheel order: each pushes the ball down along the hit
+// normal. Nothing else in a car's vehicle update reads the ball's velocity, so the pushes are recorded and applied
+// afterwards in the arena's car order, which keeps the reference's floating-point order (reference WheelRayPhase,
+// raycast_wheels_and_contact_prep.hpp:2200-2207) while the cars' updates run independently.
+struct WheelBallPushes {
+    int32_t count;
+    V3 point_bt[4], normal[4];
+};
+RG_HDI void apply_wheel_ball_pushes(BallState& ball, const WheelBallPushes& p, const TickConfig& tc) {
+    for (int k = 0; k < p.count; ++k) {
+        ball.sleeping |= 4u;
+        const V3 push_bt = -p.normal[k];
+        ball.vel_bt = ball.vel_bt + push_bt * (1.0f / tc.ball_mass);
+        ball.vel = ball.vel_bt * 50.0f;
+        ball.ang_vel = ball.ang_vel + ball_inv_inertia_bt(ball, tc.ball_mass, tc.ball_radius,
+                                                          cross(p.point_bt[k] - ball.pos_bt, push_bt));
+    }
+}
+
+RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg, const TickConfig& tc,
+                           WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, WheelBallPushes& pushes) {
+    pushes.count = 0;
     const float dt = tc.tick_dt;
     c.demo_no_contact_response = c.is_demoed ? 1 : 0;
     if (c.is_demoed) return;
@@ -771,14 +791,11 @@ RG_HDI void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg,
             if (w.is_in_contact) w.extra_pushback = 0.0f;
             if (w.is_in_contact_with_world) world_wheel_pushback(c, tc, w, f);
             if (w.is_in_contact && !w.is_in_contact_with_world && w.ground_kind == kRayHitBall) {
-                // the ray pushes the ball down (reference WheelRayPhase, :2200-2207)
-                ball.sleeping |= 4u;
-                const V3 n_bt = w.contact_normal_ws;
-                const V3 push_bt = -n_bt;
-                ball.vel_bt = ball.vel_bt + push_bt * (1.0f / tc.ball_mass);
-                ball.vel = ball.vel_bt * 50.0f;
-                ball.ang_vel = ball.ang_vel + ball_inv_inertia_bt(ball, tc.ball_mass, tc.ball_radius,
-                                                                  cross(w.contact_point_bt - ball.pos_bt, push_bt));
+                // the ray pushes the ball down (reference WheelRayPhase, :2200-2207); the caller applies the push in
+                // the arena's car order (apply_wheel_ball_pushes)
+                pushes.point_bt[pushes.count] = w.contact_point_bt;
+                pushes.normal[pushes.count] = w.contact_normal_ws;
+                ++pushes.count;
             }
             wr.extra_pushback[i] = w.extra_pushback;
             flags[i] = (w.is_in_contact ? 1u : 0u) | (w.is_in_contact_with_world ? 2u : 0u) |
