@@ -280,7 +280,8 @@ def run_ours(args, world, rank, local):
                      "note": "algorithmic state bytes per launch / launch time; the tick is FP32-issue / latency "
                              "bound (data-dependent branches, dependent loads), not HBM bound"},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps,
+        # mixed: three kernels per tick (arena begin, per-car vehicle update, arena finish); balls: one per step
+        "gpu_launches": args.steps * TICKS_PER_STEP * 3 if mixed else args.steps,
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -558,6 +558,12 @@ RG_HDI void append_velocity_rows(BallContactRows& rows, V3 normal, float restitu
 // Visits, in BVH leaf order, every triangle whose quantized bounds overlap the box [lo, hi] (Bullet units).
 template <class F>
 RG_HDI void mesh_query_box(const MeshDevice& m, V3 lo, V3 hi, F&& visit) {
+    // Clamp to the quantization bounds first, exactly as quantize_point does: the box quantizes to the same cells, a
+    // box reaching past the mesh shrinks to the part it can overlap, and a box with a non-finite coordinate (a car
+    // whose state went NaN, which the reference's EPA can produce on a flat landing) collapses onto the bounds' corner
+    // like the reference's quantized BVH walk does, instead of scanning every triangle in one lane.
+    lo = vmin(vmax(lo, m.quant.aabb_min), m.quant.aabb_max);
+    hi = vmin(vmax(hi, m.quant.aabb_min), m.quant.aabb_max);
     uint16_t qmin[3], qmax[3];
     quantize_point(m.quant, lo, 0, qmin);
     quantize_point(m.quant, hi, 1, qmax);
