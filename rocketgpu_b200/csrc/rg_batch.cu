@@ -90,6 +90,7 @@ struct rg_batch {
     DeviceArray<rg::Broadphase> broadphase;    // per arena: sweep history and manifold list
     DeviceArray<rg::CarWorldScratch> car_world;  // per car slot: the car/mesh manifold
     DeviceArray<rg::BallCarScratch> ball_car;     // per car slot: the car/ball manifold
+    DeviceArray<rg::CarCarManifold> car_pairs;   // per arena: max_cars * (max_cars - 1) / 2 retained car-car manifolds
     DeviceArray<rg::CarTickRecord> car_records;  // per car slot: this tick's record of the car's own update
     DeviceArray<rg::ArenaTickSnap> arena_snaps;  // per arena: the ball's velocities at this tick's start
     // Step order: arenas sorted by car count (so a warp's arenas take the same loops), and the active car slots of
@@ -105,6 +106,7 @@ struct rg_batch {
     std::vector<int32_t> host_car_count;
     std::vector<int32_t> host_arena_order, host_active_cars;
     int launch_threads = 32;
+    int pair_slots = 0;
 };
 
 namespace {
@@ -208,6 +210,9 @@ struct CarTickArgs {
     rg::BallCarScratch* ball_car;
     rg::CarTickRecord* records;
     rg::ArenaTickSnap* snaps;
+    rg::CarCarManifold* pairs;
+    const uint8_t* teams;
+    int32_t pair_slots;
     const int32_t* arena_order;
     const int32_t* active_cars;
     int32_t active_car_count;
@@ -222,6 +227,8 @@ __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e,
     A.pads = a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr;
     A.controls = a.controls ? a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base
                             : nullptr;
+    A.teams = a.teams + car_base;
+    A.pairs = a.pair_slots ? a.pairs + static_cast<size_t>(e) * a.pair_slots : nullptr;
     A.count = a.base.env_car_count[e];
     A.max_cars = a.max_cars;
     A.car_base = car_base;
@@ -240,20 +247,41 @@ __global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
     a.base.envs[e] = env;
 }
 
-// Tick part 2, one thread per active car: the car's tick start and vehicle update (four suspension rays against the
-// arena mesh and the ball, tyres, jumps, boost, air control). The ball is only read.
-__global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
+// Tick part 2, one thread per active car: the car's tick start (demolition timer and respawn, quantisation, controls,
+// jumps, dodges, boost) and the speed clamp.
+__global__ void __launch_bounds__(64) car_pre_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.active_car_count) return;
     const int idx = a.active_cars[k];
     const int e = idx / a.max_cars;
     const rg::CarControls& ctrl =
         a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
-    rg::car_tick_vehicle(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], a.base.mesh,
-                         a.records[idx]);
+    rg::RespawnCtx rc;
+    rc.seed = a.base.tc.kickoff_seed;
+    rc.env_idx = e;
+    rc.env_tick = a.base.envs[e].tick;
+    rc.car_id = static_cast<uint32_t>(idx + 1);
+    rc.team = a.teams[idx];
+    rg::car_tick_pre(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], rc, a.records[idx]);
 }
 
-// Tick part 3, one thread per arena in step order: wheel pushes on the ball, the world step, post-tick, pads, goal.
+// Tick part 3, one thread per active car: the vehicle update (four suspension rays against the arena mesh and the
+// ball, tyres, drive, air control). Arenas whose cars are within wheel reach of each other are left to part 4.
+__global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.active_car_count) return;
+    const int idx = a.active_cars[k];
+    const int e = idx / a.max_cars;
+    const int base = e * a.max_cars;
+    if (rg::arena_wheel_reach_near(a.cars + base, a.car_cfgs + base, a.base.env_car_count[e])) return;
+    const rg::CarControls& ctrl =
+        a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+    rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], a.base.mesh,
+                       rg::WheelOthers{nullptr, nullptr, 0, -1}, a.records[idx].pushes);
+}
+
+// Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
+// each other, wheel pushes on the ball, the world step, post-tick, pads, goal.
 __global__ void __launch_bounds__(32) arena_finish_kernel(CarTickArgs a, int t, int report_fields) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
@@ -291,6 +319,9 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     a.car_world = b->car_world.ptr;
     a.ball_car = b->ball_car.ptr;
     a.records = b->car_records.ptr;
+    a.pairs = b->car_pairs.ptr;
+    a.teams = b->teams.ptr;
+    a.pair_slots = b->pair_slots;
     a.snaps = b->arena_snaps.ptr;
     a.arena_order = b->arena_order.ptr;
     a.active_cars = b->active_cars.ptr;
@@ -298,7 +329,7 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     return a;
 }
 
-// Arenas with cars: three launches per tick (arena begin, per-car vehicle update, arena finish).
+// Arenas with cars: four launches per tick (arena begin, per-car tick start, per-car vehicle update, arena finish).
 void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s) {
     if (b->env_count == 0) return;
     const CarTickArgs a = car_tick_args(b, controls, stride);
@@ -307,6 +338,7 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     const int car_blocks = (b->active_car_count + 63) / 64;
     for (int t = 0; t < ticks; ++t) {
         arena_begin_kernel<<<blocks, threads, 0, s>>>(a, t);
+        if (car_blocks) car_pre_kernel<<<car_blocks, 64, 0, s>>>(a, t);
         if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s>>>(a, t);
         arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, t + 1 == ticks ? 1 : 0);
     }
@@ -325,6 +357,7 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
         a.car_world[car_base + k].count = 0;
         a.ball_car[car_base + k].count = 0;
     }
+    for (int k = 0; k < a.pair_slots; ++k) a.pairs[static_cast<size_t>(e) * a.pair_slots + k].count = 0;
     rg::reset_env_to_kickoff(e, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
                              a.car_cfgs + car_base, controls + car_base,
                              a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
@@ -332,6 +365,7 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
 }
 
 void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
+    b->tc.kickoff_seed = seed;  // demolished cars draw their respawn spot from the last kickoff seed
     CarTickArgs a = car_tick_args(b, nullptr, 0);
     a.pads = b->pads.ptr;
     reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed);
@@ -397,6 +431,12 @@ rg::TickConfig resolve_tick_config(const rg_sim_config& c) {
     t.frame_frac = 0.5f;
     t.enable_scoring = c.enable_scoring;
     t.enable_boost_pads = c.enable_boost_pads;
+    t.enable_car_car = c.enable_car_car_collisions;
+    t.enable_demos = c.enable_demos;
+    t.enable_team_demos = 0;
+    t.bump_force_scale = 1.0f;
+    t.bump_cooldown_time = 0.25f;
+    t.kickoff_seed = 0;
     t.max_cars = c.max_cars_per_env;
     t.pad_count = 34;
     t.car_mass = c.car_mass;
@@ -573,6 +613,12 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         if (cap) check(cudaMemset(b->car_world.ptr, 0, cap * sizeof(rg::CarWorldScratch)), "car manifolds");
         b->ball_car.alloc(cap);
         if (cap) check(cudaMemset(b->ball_car.ptr, 0, cap * sizeof(rg::BallCarScratch)), "car-ball manifolds");
+        b->pair_slots = b->max_cars * (b->max_cars - 1) / 2;
+        b->car_pairs.alloc(static_cast<size_t>(b->env_count) * b->pair_slots);
+        if (b->pair_slots)
+            check(cudaMemset(b->car_pairs.ptr, 0, static_cast<size_t>(b->env_count) * b->pair_slots *
+                                                      sizeof(rg::CarCarManifold)),
+                  "car-car manifolds");
         b->car_records.alloc(cap);
         b->arena_snaps.alloc(b->env_count);
         b->arena_order.alloc(b->env_count);

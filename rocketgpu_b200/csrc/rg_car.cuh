@@ -23,6 +23,7 @@ constexpr float kSteerDegToRad = 0.01745329238474369f;  // reference constants.h
 constexpr float kWheelSuspensionSubtraction = 2.5f;
 constexpr uint64_t kNoTick = ~0ull;
 constexpr int kKickoffSpawnOverridePlus1 = 5;  // reference rocketgpu.h:529
+constexpr int kRespawnOffsetOverridePlus1 = 128;  // reference rocketgpu.h:533
 
 // Pre-tick flags the vehicle update reads back (reference env_step.hpp:2978-2979).
 constexpr uint8_t kCalPreAirJumpStarted = 1, kCalPreFlipStarted = 2, kCalPreFlipVelChanged = 4,

@@ -83,6 +83,10 @@ struct TickConfig {
     float car_air_damp_pitch, car_air_damp_yaw, car_air_damp_roll;
     float boost_pad_cooldown_small, boost_pad_cooldown_big, demo_respawn_time;
     float arena_friction, arena_restitution;
+    // car/car contacts (reference MutatorConfig: bump_force_scale 1, bump_cooldown_time 0.25, team demos off)
+    uint8_t enable_car_car, enable_demos, enable_team_demos;
+    float bump_force_scale, bump_cooldown_time;
+    uint64_t kickoff_seed;  // the last reset_to_kickoff seed: demolished cars' respawn draw (reference Impl::seed)
 };
 
 }  // namespace rg

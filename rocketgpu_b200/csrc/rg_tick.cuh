@@ -10,9 +10,11 @@
 #include "rg_ball_car.cuh"
 #include "rg_ball_world.cuh"
 #include "rg_broadphase.cuh"
+#include "rg_car_car.cuh"
 #include "rg_car_world.cuh"
 #include "rg_math.cuh"
 #include "rg_pads.cuh"
+#include "rg_reset.cuh"
 #include "rg_vehicle.cuh"
 #include "rg_mesh.h"
 #include "rg_state.cuh"
@@ -259,6 +261,8 @@ struct ArenaCars {
     const CarConfig* cfgs;
     PadState* pads;
     const CarControls* controls;
+    const uint8_t* teams;
+    CarCarManifold* pairs;  // the arena's retained car-car manifolds, slot car_pair_slot(lo, hi)
     int count, max_cars, car_base;
 };
 
@@ -310,22 +314,97 @@ RG_HDI void update_game_visit_order(EnvState& env, const CarState* cars, int cou
 // fields, internal clocks after a state set, the demolition timer, the tick-start quantization, the pre-physics
 // control logic and the rigid-body speed clamp.
 // Returns the car's uu velocity right after the tick-start quantisation.
-RG_HDI V3 car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w) {
+// Where a demolished car comes back: the respawn spot chosen by the arena's respawn draw (reference
+// RespawnStartIndex, RespawnPlace, RespawnCar, KickoffSpawnCar, arena_ball.hpp:3092-3177).
+struct RespawnCtx {
+    uint64_t seed;  // the batch's last kickoff seed
+    int env_idx;
+    uint32_t env_tick, car_id;
+    uint8_t team;
+};
+RG_HDI int respawn_start_index(uint64_t seed, int env_idx, uint64_t tick, uint32_t car_id) {
+    uint32_t st = mix_seed(seed ^ (tick * 0x9e3779b97f4a7c15ull), env_idx, static_cast<int>(car_id * 0x45d9f3bu));
+    st = rng_advance(st);
+    return static_cast<int>(static_cast<float>((st >> 16) & 0x7fffu) * (1.0f / 32768.0f) * 4.0f);
+}
+RG_HDI SpawnPos soccar_respawn_spawn(int i) {
+    switch (i) {
+        case 0: return SpawnPos{-2304.0f, -4608.0f, kPiF * 0.5f};
+        case 1: return SpawnPos{-2688.0f, -4608.0f, kPiF * 0.5f};
+        case 2: return SpawnPos{2304.0f, -4608.0f, kPiF * 0.5f};
+        default: return SpawnPos{2688.0f, -4608.0f, kPiF * 0.5f};
+    }
+}
+RG_HDI void respawn_car(CarState& c, const CarConfig& cfg, const TickConfig& tc, const RespawnCtx& rc) {
+    const int team = rc.team;
+    int slot = -1, offset_dir = -1;
+    if (c.respawn_slot_override_plus1 >= kRespawnOffsetOverridePlus1 &&
+        c.respawn_slot_override_plus1 < kRespawnOffsetOverridePlus1 + 32) {
+        offset_dir = (c.respawn_slot_override_plus1 - kRespawnOffsetOverridePlus1) & 7;
+        slot = ((c.respawn_slot_override_plus1 - kRespawnOffsetOverridePlus1) >> 3) & 3;
+        c.respawn_slot_override_plus1 = 0;
+    } else if (c.respawn_slot_override_plus1 != 0) {
+        slot = c.respawn_slot_override_plus1 - 1;
+        c.respawn_slot_override_plus1 = 0;
+    }
+    if (slot < 0) slot = respawn_start_index(rc.seed, rc.env_idx, static_cast<uint64_t>(rc.env_tick), rc.car_id);
+    if (offset_dir < 0 && slot >= kKickoffSpawnOverridePlus1 - 1) {
+        const uint16_t driving_disabled = c.driving_disabled;
+        place_car_at_kickoff_spawn(c, team, soccar_kickoff_spawn(slot - (kKickoffSpawnOverridePlus1 - 1)), cfg.spawn_z,
+                                   tc.boost_spawn_amount);
+        c.driving_disabled = driving_disabled;
+        c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
+        return;
+    }
+    SpawnPos spawn = soccar_respawn_spawn(slot % 4);
+    if (offset_dir >= 0) {
+        const bool blue = team == 0;
+        const float fx = 0.0f, fy = blue ? 1.0f : -1.0f;
+        float gx = spawn.x, gy = blue ? spawn.y : -spawn.y;
+        constexpr float k = 0.70710677f;
+        const int d = offset_dir & 7;
+        const float ux = d == 0 ? 1.0f : (d == 1 || d == 7) ? k : (d == 2 || d == 6) ? 0.0f : (d == 3 || d == 5) ? -k : -1.0f;
+        const float uy = (d == 0 || d == 4) ? 0.0f : (d == 1 || d == 3) ? k : d == 2 ? 1.0f : d == 6 ? -1.0f : -k;
+        gx += 192.0f * (fx * ux - fy * uy);
+        gy += 192.0f * (fx * uy + fy * ux);
+        spawn.x = gx;
+        spawn.y = blue ? gy : -gy;
+    }
+    // reference PlaceCarAtRespawnSpawn (arena_ball.hpp:2562-2577): x is not mirrored for orange
+    const float y = team == 0 ? spawn.y : -spawn.y;
+    const float yaw = spawn.yaw + (team == 0 ? 0.0f : kPiF);
+    car_set_pos_bt(c, V3{spawn.x, y, cfg.spawn_z} * kUuToBt);
+    c.rot = quat_from_yaw(wrap_angle(yaw));
+    seed_car_basis_from_spawn(c, spawn_yaw_rotator_units(spawn.yaw), team == 1);
+    reset_car_common(c, tc.boost_spawn_amount);
+    c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
+    c.is_on_ground = 0;
+}
+
+RG_HDI V3 car_pre_tick(CarState& c, const CarControls& k, const CarConfig& cfg, const TickConfig& tc, WheelRuntime& w,
+                       const RespawnCtx& rc) {
     c.ball_contact_this_tick = 0;
     restore_step_fields(c);
     if (c.tick_count_since_update == 0) cal_internal_timers_from_set_state(c, tc);
     if (c.just_respawned) c.just_respawned = 0;
+    bool respawned = false;
     if (c.is_demoed) {
         c.demo_respawn_timer = fmax_(0.0f, c.demo_respawn_timer - tc.tick_dt);
-        if (!(c.demo_respawn_timer <= 0.0f) && !(fmax_(0.0f, c.demo_respawn_timer - tc.tick_dt) > 0.0f) &&
-            !(c.respawn_slot_override_plus1 >= kKickoffSpawnOverridePlus1 &&
-              c.respawn_slot_override_plus1 < kKickoffSpawnOverridePlus1 + 5)) {
+        if (c.demo_respawn_timer <= 0.0f) {
+            respawn_car(c, cfg, tc, rc);
+            respawned = true;
+        } else if (!(fmax_(0.0f, c.demo_respawn_timer - tc.tick_dt) > 0.0f) &&
+                   !(c.respawn_slot_override_plus1 >= kKickoffSpawnOverridePlus1 &&
+                     c.respawn_slot_override_plus1 < kKickoffSpawnOverridePlus1 + 5)) {
             c.boost = tc.boost_spawn_amount;
             c.boost_amount = c.boost / 100.0f;
         }
     }
+    const Q4 spawn_rot = c.rot;
     c.tick_start_pos_bt = c.pos_bt;
     car_tick_start_quantize(c, tc);
+    if (respawned)
+        spawn_inertia_basis(spawn_rot, c.tick_start_basis_forward, c.tick_start_basis_right, c.tick_start_basis_up);
     const Q4 snap_rot = c.rot;
     const V3 snap_vel = c.vel;
     cal_flip_z_damp_prepass(c, tc);
@@ -377,19 +456,24 @@ RG_HDI bool car_predictive_hit(const CarState& c, const CarConfig& cfg, const Me
 // Rows act on their bodies' velocity deltas (a car-ball row on both, reference
 // SolveBallVelocity{Normal,Friction}RowWithAccumulators, arena_geometry.hpp:2618-2750); one iteration count (stop
 // when nothing changed) covers all.
-RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list,
-                                   int n_list, V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
-    constexpr int kMax = kMaxBallVelRows + kMaxBallCarRows + kMaxCarWorldRows;
+RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, CarCarRows& pr,
+                                   const BpEntry* list, int n_list, V3& ball_dl, V3& ball_da, V3* car_dl, V3* car_da) {
+    constexpr int kMax = kMaxBallVelRows + kMaxBallCarRows + kMaxCarWorldRows + kMaxPairRows;
     uint8_t nb[kMax], ni[kMax], fb[kMax], fi[kMax];
     int nn = 0, nf = 0;
     const int bcn = bc.nv, bcf = bc.nf;
     const int wn = cr.nv, bn = bcn + br.vel_count, wf = cr.nf, bf = bcf + br.fric_count;
+    const int pn = pr.nv, pf = pr.nf;
     // combined ball index: car-ball rows first
     auto ball_fric_normal = [&](int f) { return f < bcf ? bc.fric[f].normal_row : br.fric[f - bcf].normal_row + bcn; };
     auto ball_applied = [&](int r) { return r < bcn ? bc.vel[r].applied : br.vel[r - bcn].applied; };
-    if (wn + bn <= 1 && wf + bf <= 1) {
+    if (wn + pn + bn <= 1 && wf + pf + bf <= 1) {
         if (wn == 1) {
             nb[0] = 0;
+            ni[0] = 0;
+            nn = 1;
+        } else if (pn == 1) {
+            nb[0] = 1;
             ni[0] = 0;
             nn = 1;
         } else if (bn == 1) {
@@ -401,13 +485,17 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
             fb[0] = 0;
             fi[0] = 0;
             nf = 1;
+        } else if (pf == 1) {
+            fb[0] = 1;
+            fi[0] = 0;
+            nf = 1;
         } else if (bf == 1) {
             fb[0] = 2;
             fi[0] = 0;
             nf = 1;
         }
     } else {
-        uint64_t wused = 0, bused = 0;
+        uint64_t wused = 0, bused = 0, pused = 0;
         for (int e = 0; e < n_list; ++e) {
             const uint32_t key = list[e].key;
             const int kind = bp_kind(key);
@@ -420,6 +508,15 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
                     if (cr.vel[r].body != body || cr.vel[r].tag != tag) continue;
                     wused |= 1ull << r;
                     nb[nn] = 0;
+                    ni[nn++] = static_cast<uint8_t>(r);
+                }
+            } else if (kind == 3) {
+                const int lo = bp_body_a(key), hi = bp_body_b(key);
+                for (int r = 0; r < pn; ++r) {
+                    const int ra = pr.vel[r].a, rb = pr.vel[r].b;
+                    if (((pused >> r) & 1ull) || (ra < rb ? ra : rb) != lo || (ra < rb ? rb : ra) != hi) continue;
+                    pused |= 1ull << r;
+                    nb[nn] = 1;
                     ni[nn++] = static_cast<uint8_t>(r);
                 }
             } else if (kind == 1) {
@@ -444,18 +541,30 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
                 nb[nn] = 0;
                 ni[nn++] = static_cast<uint8_t>(r);
             }
+        for (int r = 0; r < pn; ++r)
+            if (!((pused >> r) & 1ull)) {
+                nb[nn] = 1;
+                ni[nn++] = static_cast<uint8_t>(r);
+            }
         for (int r = 0; r < bn; ++r)
             if (!((bused >> r) & 1ull)) {
                 nb[nn] = 2;
                 ni[nn++] = static_cast<uint8_t>(r);
             }
-        uint64_t wfu = 0, bfu = 0;
+        uint64_t wfu = 0, bfu = 0, pfu = 0;
         for (int k = 0; k < nn; ++k) {
             if (nb[k] == 0) {
                 for (int f = 0; f < wf; ++f)
                     if (!((wfu >> f) & 1ull) && cr.fric[f].normal_row == ni[k]) {
                         wfu |= 1ull << f;
                         fb[nf] = 0;
+                        fi[nf++] = static_cast<uint8_t>(f);
+                    }
+            } else if (nb[k] == 1) {
+                for (int f = 0; f < pf; ++f)
+                    if (!((pfu >> f) & 1ull) && pr.fric[f].normal_row == ni[k]) {
+                        pfu |= 1ull << f;
+                        fb[nf] = 1;
                         fi[nf++] = static_cast<uint8_t>(f);
                     }
             } else {
@@ -470,6 +579,11 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
         for (int f = 0; f < wf; ++f)
             if (!((wfu >> f) & 1ull)) {
                 fb[nf] = 0;
+                fi[nf++] = static_cast<uint8_t>(f);
+            }
+        for (int f = 0; f < pf; ++f)
+            if (!((pfu >> f) & 1ull)) {
+                fb[nf] = 1;
                 fi[nf++] = static_cast<uint8_t>(f);
             }
         for (int f = 0; f < bf; ++f)
@@ -573,6 +687,32 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
                 car_dl[r.car] = car_dl[r.car] + ((-r.normal) * r.car_inv_mass) * di;
                 car_da[r.car] = car_da[r.car] + r.car_ang * di;
                 changed = true;
+            } else if (nb[k] == 1) {
+                // a pair row: car a along normal_a, car b along -normal_a (reference SolveSharedCarVelocityNormalRow)
+                PairVelRow& r = pr.vel[ni[k]];
+                const V3 nbv = -r.normal_a;
+                const float dva = bt_dot(r.normal_a, car_dl[r.a]) + bt_dot(r.rel_a_cross, car_da[r.a]);
+                const float dvb = bt_dot(nbv, car_dl[r.b]) + bt_dot(r.rel_b_cross, car_da[r.b]);
+                const float before = r.applied;
+                float di = r.rhs;
+                di = di - dvb * r.jac;
+                di = di - dva * r.jac;
+                const float sum = before + di;
+                if (sum < 0.0f) {
+                    di = -before;
+                    r.applied = 0.0f;
+                } else {
+                    r.applied = sum;
+                }
+                if (di == 0.0f) {
+                    changed = (f2u(before) != f2u(r.applied)) || changed;
+                    continue;
+                }
+                car_dl[r.a] = car_dl[r.a] + (r.normal_a * r.inv_mass) * di;
+                car_da[r.a] = car_da[r.a] + r.ang_a * di;
+                car_dl[r.b] = car_dl[r.b] + (nbv * r.inv_mass) * di;
+                car_da[r.b] = car_da[r.b] + r.ang_b * di;
+                changed = true;
             } else if (nb[k] == 2) {
                 BallVelRow& r = br.vel[ni[k] - bcn];
                 changed = solve_normal(r.normal, r.rel_cross, r.ang, r.inv_mass, r.jac_inv, r.rhs, r.applied, ball_dl,
@@ -592,6 +732,37 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
                 changed = solve_pair(r.tangent, r.rel_ball_cross, r.ball_ang, r.ball_inv_mass, r.rel_car_cross,
                                      r.car_ang, r.car_inv_mass, r.jac, r.rhs, -maxi, maxi, r.applied, ball_dl, ball_da,
                                      car_dl[r.car], car_da[r.car]) || changed;
+            } else if (fb[k] == 1) {
+                PairFricRow& r = pr.fric[fi[k]];
+                const float total = pr.vel[r.normal_row].applied;
+                if (total <= 0.0f) continue;
+                const float maxi = r.friction * total;
+                const V3 tb = -r.tangent_a;
+                float di = r.rhs;
+                const float dvb = bt_dot(tb, car_dl[r.b]) + bt_dot(r.rel_b_cross, car_da[r.b]);
+                di = di - dvb * r.jac;
+                const float dva = bt_dot(r.tangent_a, car_dl[r.a]) + bt_dot(r.rel_a_cross, car_da[r.a]);
+                di = di - dva * r.jac;
+                const float before = r.applied;
+                const float sum = before + di;
+                if (sum < -maxi) {
+                    di = -maxi - before;
+                    r.applied = -maxi;
+                } else if (sum > maxi) {
+                    di = maxi - before;
+                    r.applied = maxi;
+                } else {
+                    r.applied = sum;
+                }
+                if (di == 0.0f) {
+                    changed = (f2u(before) != f2u(r.applied)) || changed;
+                    continue;
+                }
+                car_dl[r.a] = car_dl[r.a] + (r.tangent_a * r.inv_mass) * di;
+                car_da[r.a] = car_da[r.a] + r.ang_a * di;
+                car_dl[r.b] = car_dl[r.b] + (tb * r.inv_mass) * di;
+                car_da[r.b] = car_da[r.b] + r.ang_b * di;
+                changed = true;
             } else if (fb[k] == 2) {
                 BallFricRow& r = br.fric[fi[k] - bcf];
                 const float total = ball_applied(r.normal_row + bcn);
@@ -615,18 +786,48 @@ RG_NOINL void unified_velocity_solve(BallContactRows& br, BallCarRows& bc, CarWo
 // SolveUnifiedBallSplitRow, :3523-3600). Returns the ball's push velocity; the cars' push and turn velocities come
 // back in `car_push` / `car_turn`, `car_bt` telling which cars had Bullet-unit rows (every row here carries Bullet
 // units, so a car is in Bullet units when any of its arena or car-ball rows exists, MarkBtSplitAccumulators).
-RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, const BpEntry* list, int n_list,
-                              V3* car_push, V3* car_turn, bool* car_bt, int count) {
-    constexpr int kMax = kMaxBallSplitRows + kMaxBallCarRows + kMaxCarWorldRows;
-    for (int i = 0; i < count; ++i) car_bt[i] = false;
-    for (int r = 0; r < cr.ns; ++r) car_bt[cr.split[r].body] = true;
-    for (int r = 0; r < bc.ns; ++r) car_bt[bc.split[r].car] = true;
+RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRows& cr, CarCarRows& pr,
+                              const BpEntry* list, int n_list, V3* car_push, V3* car_turn, bool* car_bt, int count) {
+    constexpr int kMax = kMaxBallSplitRows + kMaxBallCarRows + kMaxCarWorldRows + kMaxPairRows;
+    // Bullet-unit accumulators (reference MarkBtSplitAccumulators, arena_geometry.hpp:3317-3431): a car is in
+    // Bullet units when one of its split rows exists and none of the rows reaching it (through pair and car-ball rows)
+    // lacks Bullet-unit terms; only a pair row whose Bullet-unit penetration rounds to zero lacks them.
+    bool touched[8], blocked[8];
+    for (int i = 0; i < 8; ++i) touched[i] = blocked[i] = false;
+    for (int r = 0; r < cr.ns; ++r) touched[cr.split[r].body] = true;
+    for (int r = 0; r < pr.ns; ++r) {
+        touched[pr.split[r].a] = touched[pr.split[r].b] = true;
+        if (!pr.split[r].has_bt) blocked[pr.split[r].a] = blocked[pr.split[r].b] = true;
+    }
+    for (int r = 0; r < bc.ns; ++r) touched[bc.split[r].car] = true;
+    if (pr.ns > 0 || bc.ns > 0 || br.split_count > 0) {
+        bool ball_blocked = false;
+        for (int pass = 0; pass < 8; ++pass) {
+            bool changed = false;
+            for (int r = 0; r < pr.ns; ++r) {
+                const int a = pr.split[r].a, b = pr.split[r].b;
+                if (blocked[a] != blocked[b]) {
+                    blocked[a] = blocked[b] = true;
+                    changed = true;
+                }
+            }
+            for (int r = 0; r < bc.ns; ++r) {
+                const int o = bc.split[r].car;
+                if (blocked[o] != ball_blocked) {
+                    blocked[o] = ball_blocked = true;
+                    changed = true;
+                }
+            }
+            if (!changed) break;
+        }
+    }
+    for (int i = 0; i < count && i < 8; ++i) car_bt[i] = touched[i] && !blocked[i];
     const int bcs = bc.ns;
-    const int ws = cr.ns, bs = bcs + br.split_count;
+    const int ws = cr.ns, ps = pr.ns, bs = bcs + br.split_count;
     uint8_t ob[kMax], oi[kMax];
     int no = 0;
-    if (n_list > 0 && ws + bs > 1) {
-        uint64_t wused = 0, bused = 0;
+    if (n_list > 0 && ws + ps + bs > 1) {
+        uint64_t wused = 0, bused = 0, pused = 0;
         for (int e = 0; e < n_list; ++e) {
             const uint32_t key = list[e].key;
             const int kind = bp_kind(key);
@@ -638,6 +839,15 @@ RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRo
                     if (((wused >> r) & 1ull) || cr.split[r].body != body || cr.split[r].tag != tag) continue;
                     wused |= 1ull << r;
                     ob[no] = 0;
+                    oi[no++] = static_cast<uint8_t>(r);
+                }
+            } else if (kind == 3) {
+                const int lo = bp_body_a(key), hi = bp_body_b(key);
+                for (int r = 0; r < ps; ++r) {
+                    const int ra = pr.split[r].a, rb = pr.split[r].b;
+                    if (((pused >> r) & 1ull) || (ra < rb ? ra : rb) != lo || (ra < rb ? rb : ra) != hi) continue;
+                    pused |= 1ull << r;
+                    ob[no] = 1;
                     oi[no++] = static_cast<uint8_t>(r);
                 }
             } else if (kind == 1) {
@@ -663,6 +873,11 @@ RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRo
                 ob[no] = 0;
                 oi[no++] = static_cast<uint8_t>(r);
             }
+        for (int r = 0; r < ps; ++r)
+            if (!((pused >> r) & 1ull)) {
+                ob[no] = 1;
+                oi[no++] = static_cast<uint8_t>(r);
+            }
         for (int r = 0; r < bs; ++r)
             if (!((bused >> r) & 1ull)) {
                 ob[no] = 2;
@@ -671,6 +886,10 @@ RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRo
     } else {
         for (int r = 0; r < ws; ++r) {
             ob[no] = 0;
+            oi[no++] = static_cast<uint8_t>(r);
+        }
+        for (int r = 0; r < ps; ++r) {
+            ob[no] = 1;
             oi[no++] = static_cast<uint8_t>(r);
         }
         for (int r = 0; r < bs; ++r) {
@@ -708,6 +927,34 @@ RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRo
                 p = p + ((-r.normal) * r.car_inv_mass) * di;
                 t = t + r.car_ang * di;
                 changed = true;
+            } else if (ob[k] == 1) {
+                // a pair row in Bullet units (reference SolveSharedCarSplitRow)
+                PairSplitRow& r = pr.split[oi[k]];
+                if (r.rhs == 0.0f) continue;
+                V3& pa = car_push[r.a];
+                V3& ta = car_turn[r.a];
+                V3& pb = car_push[r.b];
+                V3& tb = car_turn[r.b];
+                const V3 nbv = -r.normal_a;
+                const float before = r.applied;
+                float di = r.rhs;
+                const float dva = bt_dot(r.normal_a, pa) + bt_dot(r.rel_a_cross, ta);
+                di -= (bt_dot(nbv, pb) + bt_dot(r.rel_b_cross, tb)) * r.jac;
+                di -= dva * r.jac;
+                const float sum = r.applied + di;
+                if (sum < 0.0f) {
+                    di = 0.0f - r.applied;
+                    r.applied = 0.0f;
+                } else {
+                    r.applied = sum;
+                }
+                if (di != 0.0f) {
+                    pa = pa + (r.normal_a * r.inv_mass) * di;
+                    ta = ta + r.ang_a * di;
+                    pb = pb + (nbv * r.inv_mass) * di;
+                    tb = tb + r.ang_b * di;
+                }
+                changed = di != 0.0f || f2u(before) != f2u(r.applied) || changed;
             } else if (ob[k] == 2) {
                 BallSplitRow& r = br.split[oi[k] - bcs];
                 const float before = r.applied_bt;
@@ -753,6 +1000,25 @@ RG_NOINL V3 unified_split_solve(BallContactRows& br, BallCarRows& bc, CarWorldRo
         if (!changed) break;
     }
     return push;
+}
+
+// The car's hitbox AABB against the ball's (radius + 0.08 bt) in Bullet units (reference BallCarRetainedPairOverlaps).
+RG_HDI bool ball_car_box_overlaps(const BallState& b, const CarState& car, const CarConfig& cfg, const TickConfig& c,
+                                  bool allow_midtick_demo) {
+    if ((!allow_midtick_demo && car.is_demoed) || car.just_respawned) return false;
+    V3 ax{1.0f, 0.0f, 0.0f}, ay{0.0f, 1.0f, 0.0f}, az{0.0f, 0.0f, 1.0f};
+    car_basis(car, ax, ay, az);
+    const V3 half = car_box_half_bt(cfg);
+    const V3 off = cfg.hitbox_offset * (1.0f / 50.0f);
+    const V3 center = car.pos_bt + ax * off.x + ay * off.y + az * off.z;
+    const V3 ext{fabs_(ax.x) * half.x + fabs_(ay.x) * half.y + fabs_(az.x) * half.z,
+                 fabs_(ax.y) * half.x + fabs_(ay.y) * half.y + fabs_(az.y) * half.z,
+                 fabs_(ax.z) * half.x + fabs_(ay.z) * half.y + fabs_(az.z) * half.z};
+    const float r = c.ball_radius * (1.0f / 50.0f) + 0.08f;
+    const V3 bmin = b.pos_bt - V3{r, r, r}, bmax = b.pos_bt + V3{r, r, r};
+    const V3 cmin = center - ext, cmax = center + ext;
+    return !(cmin.x > bmax.x || cmax.x < bmin.x || cmin.y > bmax.y || cmax.y < bmin.y || cmin.z > bmax.z ||
+             cmax.z < bmin.z);
 }
 
 // One arena's world step with cars (reference WorldStepSoccar, env_step.hpp:4727-5623, on the path a custom-mesh
@@ -812,6 +1078,57 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
     BpEntry list[kBpMaxEntries];
     const int n_list = bp_build_manifold_list(bp, proxies, body_count, mesh.aabb_min, mesh.aabb_max, pred_mask,
                                               ball_sleeping && !vehicle_woke, list);
+    // car/car contacts (reference env_step.hpp:4916-5042): pairs in the built manifold list's order, then the remaining
+    // pairs in slot order; a pair whose retained manifold is empty and whose cars are apart or inactive is skipped
+    uint32_t car_car_touched = 0u;
+    CarCarRows pr;
+    pr.nv = pr.nf = pr.ns = 0;
+    if (c.enable_car_car && count >= 2 && A.pairs) {
+        const uint32_t reject = car_car_reject_mask(A.cars, A.cfgs, A.pairs, count);
+        const int pc = count < 8 ? count : 8;
+        const uint32_t all = pc >= 2 ? (1u << (pc * (pc - 1) / 2)) - 1u : 0u;
+        if ((reject & all) != all) {
+            int8_t oi[28], oj[28];
+            int no = 0;
+            uint32_t listed = 0u;
+            // the list as built, before its island sort (the reference sorts after the car pairs, env_step.hpp:5186)
+            const int n_built = bp.manifold_count < kBpMaxEntries ? bp.manifold_count : kBpMaxEntries;
+            for (int e = 0; e < n_built; ++e) {
+                const uint32_t key = bp.manifolds[e];
+                if (bp_kind(key) != 3) continue;
+                const int x = bp_body_a(key), y = bp_body_b(key);
+                const int pi = x < y ? x : y, pj = x < y ? y : x;
+                if (pi < 0 || pj >= count || pj >= 8 || pi == pj) continue;
+                const uint32_t bit = 1u << car_pair_slot(pi, pj);
+                if (listed & bit) continue;
+                listed |= bit;
+                if (reject & bit) continue;
+                oi[no] = static_cast<int8_t>(pi);
+                oj[no] = static_cast<int8_t>(pj);
+                ++no;
+            }
+            for (int pi = 0; pi < count && pi < 8; ++pi)
+                for (int pj = pi + 1; pj < count && pj < 8; ++pj) {
+                    const uint32_t bit = 1u << car_pair_slot(pi, pj);
+                    if ((listed & bit) || (reject & bit)) continue;
+                    if (no < 28) {
+                        oi[no] = static_cast<int8_t>(pi);
+                        oj[no] = static_cast<int8_t>(pj);
+                        ++no;
+                    }
+                }
+            for (int po = 0; po < no; ++po) {
+                const int i = oi[po], j = oj[po];
+                car_car_touched |= (1u << i) | (1u << j);
+                // Bullet's body order in the pair: the car whose sweep handle is lower is body 0
+                const bool i_body0 = bp.body_handle[i + 1] <= bp.body_handle[j + 1];
+                const int a = i_body0 ? j : i, b2 = i_body0 ? i : j;
+                car_car_resolve(A.cars[a], static_cast<uint32_t>(A.car_base + a + 1), A.teams[a], A.cfgs[a], A.cars[b2],
+                                static_cast<uint32_t>(A.car_base + b2 + 1), A.teams[b2], A.cfgs[b2], c, pre[a], pre[b2],
+                                snap.car_start_vel[a], snap.car_start_vel[b2], a, b2, A.pairs[car_pair_slot(i, j)], pr);
+            }
+        }
+    }
     // car-ball contacts, in slot order: a car whose box AABB meets the ball's takes part (reference
     // env_step.hpp:5045-5133; a car with no valid proxy is demolished and never overlaps,
     // BallCarRetainedPairOverlaps)
@@ -821,10 +1138,15 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
         const BpProxy& pb = proxies[0];
         const BpProxy& pc = proxies[i + 1];
         CarState& car = A.cars[i];
-        const bool overlaps = i + 1 < body_count && pc.valid != 0 && !car.just_respawned &&
-                              !(pc.child_min.x > pb.child_max.x || pc.child_max.x < pb.child_min.x ||
-                                pc.child_min.y > pb.child_max.y || pc.child_max.y < pb.child_min.y ||
-                                pc.child_min.z > pb.child_max.z || pc.child_max.z < pb.child_min.z);
+        // a car touched by a car pair tests its current box instead of its swept proxy
+        // (reference BallCarRetainedPairOverlaps, triangle_and_carcar.hpp:1658-1698)
+        const bool overlaps =
+            ((car_car_touched >> i) & 1u)
+                ? ball_car_box_overlaps(b, car, A.cfgs[i], c, pre[i].is_demoed == 0)
+                : (i + 1 < body_count && pc.valid != 0 && !car.just_respawned &&
+                   !(pc.child_min.x > pb.child_max.x || pc.child_max.x < pb.child_min.x ||
+                     pc.child_min.y > pb.child_max.y || pc.child_max.y < pb.child_min.y ||
+                     pc.child_min.z > pb.child_max.z || pc.child_max.z < pb.child_min.z));
         if (!overlaps) {
             bcs[i].count = 0;
             continue;
@@ -900,11 +1222,11 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
         }
     }
     // velocity solve
-    if (rows.vel_count || rows.fric_count || cr.nv || cr.nf || bc.nv || bc.nf) {
+    if (rows.vel_count || rows.fric_count || cr.nv || cr.nf || bc.nv || bc.nf || pr.nv || pr.nf) {
         V3 dl{0, 0, 0}, da{0, 0, 0};
         V3 cdl[8], cda[8];
         for (int i = 0; i < count; ++i) cdl[i] = cda[i] = V3{0.0f, 0.0f, 0.0f};
-        unified_velocity_solve(rows, bc, cr, list, n_list, dl, da, cdl, cda);
+        unified_velocity_solve(rows, bc, cr, pr, list, n_list, dl, da, cdl, cda);
         ball_set_vel_bt(b, solver_vel_bt + dl);
         b.ang_vel = b.ang_vel + da;
         for (int i = 0; i < count; ++i) {
@@ -913,10 +1235,10 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
         }
     }
     // position (split-impulse) solve
-    if (rows.split_count || cr.ns || bc.ns) {
+    if (rows.split_count || cr.ns || bc.ns || pr.ns) {
         V3 cpush[8], cturn[8];
         bool cbt[8];
-        const V3 push = unified_split_solve(rows, bc, cr, list, n_list, cpush, cturn, cbt, count);
+        const V3 push = unified_split_solve(rows, bc, cr, pr, list, n_list, cpush, cturn, cbt, count);
         if (!is_zero(push)) ball_set_pos_bt(b, b.pos_bt + push * sub_dt);
         for (int i = 0; i < count; ++i) {
             CarState& car = A.cars[i];
@@ -999,17 +1321,36 @@ RG_HDI void arena_tick_begin(EnvState& env, BallState& b, const ArenaCars& A, co
         for (int p = 0; p < pads_layout.count; ++p) pad_pre_tick(A.pads[p], c.tick_dt);
 }
 
-RG_HDI void car_tick_vehicle(CarState& car, const CarControls& k, const CarConfig& cfg, const TickConfig& c,
-                             WheelRuntime& w, const BallState& b, const MeshDevice& mesh, CarTickRecord& r) {
-    r.start_vel = car_pre_tick(car, k, cfg, c, w);
+RG_HDI void car_tick_pre(CarState& car, const CarControls& k, const CarConfig& cfg, const TickConfig& c,
+                         WheelRuntime& w, const RespawnCtx& rc, CarTickRecord& r) {
+    r.start_vel = car_pre_tick(car, k, cfg, c, w, rc);
     r.vel_bt = car.vel_bt;
     r.ang_vel = car.ang_vel;
-    vehicle_update(car, k, cfg, c, w, b, mesh, r.pushes);
+    r.pushes.count = 0;
+}
+
+// Whether a suspension ray of one of the arena's cars can reach another car this tick: a symmetric bound on the
+// centre distance (each car's hitbox reach plus 4 bt, which covers the wheel's offset and ray length) that every
+// thread of the arena evaluates alike. Wheels on other cars push those cars at once, so such an arena runs its
+// vehicle updates in the game's car order (arena_tick_finish); all others run them one thread per car.
+RG_HDI float car_wheel_reach_bt(const CarConfig& cfg) {
+    return (0.5f * (fabs_(cfg.hitbox_size.x) + fabs_(cfg.hitbox_size.y) + fabs_(cfg.hitbox_size.z)) +
+            fabs_(cfg.hitbox_offset.x) + fabs_(cfg.hitbox_offset.y) + fabs_(cfg.hitbox_offset.z)) *
+               kUuToBt +
+           2.0f;
+}
+RG_HDI bool arena_wheel_reach_near(const CarState* cars, const CarConfig* cfgs, int count) {
+    for (int i = 0; i < count; ++i)
+        for (int j = i + 1; j < count; ++j) {
+            const float lim = car_wheel_reach_bt(cfgs[i]) + car_wheel_reach_bt(cfgs[j]);
+            if (len2(cars[i].pos_bt - cars[j].pos_bt) <= lim * lim) return true;
+        }
+    return false;
 }
 
 RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                               BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
-                              const PadLayout& pads_layout, bool report_fields, const CarTickRecord* recs,
+                              const PadLayout& pads_layout, bool report_fields, CarTickRecord* recs,
                               const ArenaTickSnap& as) {
     const int count = A.count;
     int order[8];
@@ -1022,6 +1363,14 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     }
     snap.ball_start_vel = as.ball_start_vel;
     snap.ball_vel_bt = as.ball_vel_bt;
+    if (arena_wheel_reach_near(A.cars, A.cfgs, count)) {
+        // cars within wheel reach of each other: vehicle updates in the game's car order, wheels seeing other cars
+        for (int k = 0; k < count; ++k) {
+            const int i = order[k];
+            vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh,
+                           WheelOthers{A.cars, A.cfgs, count, i}, recs[i].pushes);
+        }
+    }
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
     world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick);

@@ -163,4 +163,39 @@ RG_HDI float ucrt_powf(float x, float y) {
     return ucrt_powf_exp(dy * log_x, sign, true);
 }
 
+// acosf as the reference computes it (reference RocketGpuUcrtAcosf, math.hpp:458-491): for |x| < 0.5 a rational
+// approximation in x^2 added to pi/2 in double, for larger |x| the half-angle identity acos(x) = 2 asin(sqrt((1-x)/2))
+// with a split square root; the coefficients are the reference's, written here as their float bit patterns.
+RG_HDI float ucrt_acosf(float x) {
+    const uint32_t ux = f2u(x);
+    const uint32_t ax = ux & 0x7fffffffu, ex = (ux >> 23) & 0xffu;
+    if (ax > 0x7f800000u) return u2f(ux | 0x400000u);
+    if (ex < 0x65u) return u2f(0x3fc90fdbu);
+    if (ex >= 0x7fu) {
+        if (x == 1.0f) return 0.0f;
+        if (x == -1.0f) return u2f(0x40490fdbu);
+        return u2f(0xffc00000u);
+    }
+    const float a = fabsf(x);
+    const bool big = ex >= 0x7eu;
+    const float z = big ? (1.0f - a) * 0.5f : a * a;
+    const float s = big ? sqrtf(z) : 0.0f;
+    float t = u2f(0x3b81ce6bu);
+    t = fmaf(-t, z, u2f(0xbc5b3fe1u));
+    t = fmaf(t, z, -u2f(0x3d678bddu));
+    t = fmaf(t, z, u2f(0x3e3c94dcu));
+    const float r = (t * z) / fmaf(-u2f(0x3f561f0du), z, u2f(0x3f8d6fa5u));
+    if (!big) {
+        const double lo = 0x1.1a62633145c07p-54 - static_cast<double>(r * x);
+        return static_cast<float>(0x1.921fb54442d18p+0 - (static_cast<double>(x) - lo));
+    }
+    if (static_cast<int32_t>(ux) < 0) {
+        const double h = (static_cast<double>(s * r) - 0x1.1a62633145c07p-54) + static_cast<double>(s);
+        return static_cast<float>(0x1.921fb54442d18p+1 - (h + h));
+    }
+    const float hi = u2f(f2u(s) & 0xffff0000u);
+    const float c = fmaf(-hi, hi, z) / (s + hi);
+    return fmaf(r, s + s, c + c) + (hi + hi);
+}
+
 }  // namespace rg

@@ -269,10 +269,179 @@ RG_HDI bool wheel_ray_vs_ball(V3 src_bt, V3 dir, float max_len, const BallState&
     return true;
 }
 
-// One suspension ray against the arena mesh and the ball (reference RayCastWheelAgainstArena, :641-845, on a
-// meshes-only arena). Other cars under a wheel are not built: those rays see only the mesh and the ball.
+// The other cars of the arena a wheel ray may land on (null `cars`: none within reach, see arena_wheel_reach_near).
+struct WheelOthers {
+    CarState* cars;
+    const CarConfig* cfgs;
+    int count, self;
+};
+
+// Distance from a point to a car's hitbox (core box plus margin) by Bullet's GJK pair detector with the Voronoi
+// simplex solver; keeps the result only when it is nearer than `out_distance` (reference WheelGjkPointBoxClosest,
+// raycast_wheels_and_contact_prep.hpp:4758-4855).
+RG_HDI bool wheel_point_box_closest(V3 point_a, V3 box_origin, V3 f, V3 r, V3 u, V3 core, float margin_in,
+                                    bool& has_result, float& out_distance, V3& out_normal) {
+    constexpr float kRelError2 = 1.0e-6f;
+    constexpr float kEps = 1.1920929e-7f;
+    const V3 offset = (point_a + box_origin) * 0.5f;
+    const V3 la = point_a - offset, lb = box_origin - offset;
+    const float margin = 0.0f + margin_in;
+    V3 axis{0.0f, 1.0f, 0.0f};
+    float sq = 1.0e18f;
+    gjk::VoronoiSimplex sx;
+    sx.reset();
+    bool check = false;
+    int iter = 0;
+    const V3 pw = V3{0.0f, 0.0f, 0.0f} + la;
+    while (true) {
+        const V3 sb{dot(f, axis), dot(r, axis), dot(u, axis)};
+        const V3 ql{sb.x >= 0.0f ? core.x : -core.x, sb.y >= 0.0f ? core.y : -core.y, sb.z >= 0.0f ? core.z : -core.z};
+        const V3 qw{(f.x * ql.x + r.x * ql.y) + u.x * ql.z + lb.x, (f.y * ql.x + r.y * ql.y) + u.y * ql.z + lb.y,
+                    (f.z * ql.x + r.z * ql.y) + u.z * ql.z + lb.z};
+        const V3 w = pw - qw;
+        const float delta = dot(axis, w);
+        if (delta > 0.0f && delta * delta > sq * 1.0e18f) {
+            check = true;
+            break;
+        }
+        if (sx.in_simplex(w)) {
+            check = true;
+            break;
+        }
+        const float f0 = sq - delta, f1 = sq * kRelError2;
+        if (f0 <= f1) {
+            check = true;
+            break;
+        }
+        sx.add(w, pw, qw);
+        if (!sx.update()) {
+            check = true;
+            break;
+        }
+        const V3 na = sx.cv;
+        if (len2(na) < kRelError2) {
+            axis = na;
+            check = true;
+            break;
+        }
+        const float prev = sq;
+        sq = len2(na);
+        if (prev - sq <= kEps * prev) {
+            check = true;
+            break;
+        }
+        axis = na;
+        if (iter++ > 1000) break;
+        if (sx.full()) break;
+    }
+    if (!check) return has_result;
+    sx.update();
+    const float l2 = len2(axis);
+    if (!(l2 > kEps * kEps)) return has_result;
+    const float rlen = 1.0f / sqrtf(l2);
+    V3 normal = axis * rlen;
+    const float distance = (1.0f / rlen) - margin;
+    if (!(distance < 0.0f || distance * distance < 1.0e18f)) return has_result;
+    const V3 hm = core + V3{margin_in, margin_in, margin_in};
+    const V3 ext{(hm.x * fabs_(f.x) + hm.y * fabs_(r.x)) + hm.z * fabs_(u.x),
+                 (hm.x * fabs_(f.y) + hm.y * fabs_(r.y)) + hm.z * fabs_(u.y),
+                 (hm.x * fabs_(f.z) + hm.y * fabs_(r.z)) + hm.z * fabs_(u.z)};
+    const V3 pos_a = ((la + V3{0.0f, 0.0f, 0.0f}) + (la - V3{0.0f, 0.0f, 0.0f})) * 0.5f;
+    const V3 pos_b = ((lb - ext) + (lb + ext)) * 0.5f;
+    if (dot(pos_a - pos_b, normal) < 0.0f) normal = normal * -1.0f;
+    if (distance < out_distance) {
+        has_result = true;
+        out_normal = normal;
+        out_distance = distance;
+    }
+    return has_result;
+}
+
+// A suspension ray against another car's hitbox: slab test in the box frame, then conservative advancement with the
+// point-box distance (reference CastWheelRayAgainstCarHitboxGjkCast, raycast_wheels_and_contact_prep.hpp:4857-4977).
+RG_HDI bool wheel_ray_vs_car_box(V3 src, V3 dir, float max_len, float max_len_bt, const CarState& o,
+                                 const CarConfig& ocfg, RayHit& out) {
+    constexpr float kRadius = 0.001f;
+    const V3 to = src + dir * max_len_bt;
+    const V3 half_raw = bullet_hitbox_size(ocfg) * (0.5f * kUuToBt);
+    const float margin = fmin_(0.1f * fmin_(half_raw.x, fmin_(half_raw.y, half_raw.z)), 0.04f);
+    const V3 inner = half_raw - V3{margin, margin, margin};
+    V3 f{1.0f, 0.0f, 0.0f}, rt{0.0f, 1.0f, 0.0f}, u{0.0f, 0.0f, 1.0f};
+    car_basis(o, f, rt, u);
+    const V3 center = o.pos_bt + rotate_via_basis(f, rt, u, ocfg.hitbox_offset * kUuToBt);
+    {
+        const float rr = len(half_raw) + max_len_bt + 1.0e-3f;
+        if (len2(center - src) > rr * rr) return false;
+    }
+    {
+        const V3 rf = src - o.pos_bt, rto = to - o.pos_bt;
+        const V3 lf{dot(rf, f), dot(rf, rt), dot(rf, u)}, lt{dot(rto, f), dot(rto, rt), dot(rto, u)};
+        const V3 off = ocfg.hitbox_offset * kUuToBt;
+        const V3 ext = inner + V3{margin, margin, margin};
+        const V3 bmin = off - ext, bmax = off + ext;
+        if ((lf.x < bmin.x && lt.x < bmin.x) || (lf.x > bmax.x && lt.x > bmax.x) || (lf.y < bmin.y && lt.y < bmin.y) ||
+            (lf.y > bmax.y && lt.y > bmax.y) || (lf.z < bmin.z && lt.z < bmin.z) || (lf.z > bmax.z && lt.z > bmax.z))
+            return false;
+        V3 d = lt - lf;
+        const float dl = len(d);
+        if (!(dl > 0.0f)) return false;
+        d = d * (1.0f / dl);
+        const float lambda_max = dot(d, lt - lf);
+        const float inv[3] = {d.x == 0.0f ? 1.0e30f : 1.0f / d.x, d.y == 0.0f ? 1.0e30f : 1.0f / d.y,
+                              d.z == 0.0f ? 1.0e30f : 1.0f / d.z};
+        const float from[3] = {lf.x, lf.y, lf.z};
+        const float lo[3] = {bmin.x, bmin.y, bmin.z}, hi[3] = {bmax.x, bmax.y, bmax.z};
+        float tmin = ((inv[0] < 0.0f ? hi[0] : lo[0]) - from[0]) * inv[0];
+        float tmax = ((inv[0] < 0.0f ? lo[0] : hi[0]) - from[0]) * inv[0];
+        for (int a = 1; a < 3; ++a) {
+            const float t0 = ((inv[a] < 0.0f ? hi[a] : lo[a]) - from[a]) * inv[a];
+            const float t1 = ((inv[a] < 0.0f ? lo[a] : hi[a]) - from[a]) * inv[a];
+            if (tmin > t1 || t0 > tmax) return false;
+            if (t0 > tmin) tmin = t0;
+            if (t1 < tmax) tmax = t1;
+        }
+        if (!(tmin < lambda_max && tmax > 0.0f)) return false;
+    }
+    const V3 rv{to.x - src.x - (center.x - center.x), to.y - src.y - (center.y - center.y),
+                to.z - src.z - (center.z - center.z)};
+    bool has = false;
+    float dist = 1.0e18f;
+    V3 n{0.0f, 0.0f, 0.0f};
+    if (!wheel_point_box_closest(src, center, f, rt, u, inner, margin, has, dist, n)) return false;
+    float lambda = 0.0f;
+    int iter = 0;
+    while (true) {
+        if (dist <= kRadius) {
+            if (-0.0f <= dot(rv, n)) return false;
+            break;
+        }
+        if (++iter > 64) return false;
+        const float nl = lambda - dist / dot(rv, n);
+        if (nl > 1.0f || nl < 0.0f || nl <= lambda) return false;
+        const float s = 1.0f - nl;
+        const V3 pa{nl * to.x + s * src.x, nl * to.y + s * src.y, nl * to.z + s * src.z};
+        const V3 bo{nl * center.x + s * center.x, nl * center.y + s * center.y, nl * center.z + s * center.z};
+        if (!wheel_point_box_closest(pa, bo, f, rt, u, inner, margin, has, dist, n)) return false;
+        lambda = nl;
+        if (!(0.0f <= dist)) break;
+    }
+    const float nl2 = len2(n);
+    if (!(nl2 > 1.0e-4f) || !(lambda < 1.0f)) return false;
+    const float il = 1.0f / sqrtf(nl2);
+    const float s = 1.0f - lambda;
+    out.t = lambda * max_len;
+    out.normal = V3{n.x * il, n.y * il, n.z * il};
+    out.point_bt = V3{s * src.x + lambda * to.x, s * src.y + lambda * to.y, s * src.z + lambda * to.z};
+    out.hit = 1;
+    out.kind = kRayHitCar;
+    out.mesh_index = -1;
+    return true;
+}
+
+// One suspension ray against the arena mesh, the arena's other cars and the ball (reference RayCastWheelAgainstArena,
+// :641-845, with CastWheelRayAgainstCars :329-421, on a meshes-only arena).
 RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& ball, const TickConfig& tc,
-                           const MeshDevice& mesh, float min_hit_dist_sq_bt) {
+                           const MeshDevice& mesh, float min_hit_dist_sq_bt, const WheelOthers& oth) {
     const float real_ray_length =
         w.suspension_rest_length + w.max_suspension_travel + w.wheel_radius - kWheelSuspensionSubtraction;
     const float real_ray_length_bt = (w.suspension_rest_length * kUuToBt + w.wheel_radius * kUuToBt) +
@@ -306,6 +475,43 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
     }
     bool hit_world = hit.hit != 0;
     int32_t ground_car_idx = -1;
+    bool selected_no_response = false;
+    if (oth.cars) {
+        RayHit best;
+        best.hit = 0;
+        best.t = 0.0f;
+        int best_idx = -1;
+        bool best_nr = false;
+        for (int i = 0; i < oth.count; ++i) {
+            if (i == oth.self) continue;
+            const CarState& o = oth.cars[i];
+            if (o.is_demoed) continue;
+            {
+                const CarConfig& ocfg = oth.cfgs[i];
+                const float reach = 0.5f * (fabs_(ocfg.hitbox_size.x) + fabs_(ocfg.hitbox_size.y) +
+                                            fabs_(ocfg.hitbox_size.z)) +
+                                    fabs_(ocfg.hitbox_offset.x) + fabs_(ocfg.hitbox_offset.y) + fabs_(ocfg.hitbox_offset.z);
+                const float rr = reach * kUuToBt + real_ray_length_bt + 1.0e-2f;
+                if (len2(o.pos_bt - w.ray_source_bt) > rr * rr) continue;
+            }
+            RayHit h;
+            if (!wheel_ray_vs_car_box(w.ray_source_bt, w.wheel_dir_ws, real_ray_length, real_ray_length_bt, o,
+                                      oth.cfgs[i], h))
+                continue;
+            if (min_hit_dist_sq_bt > 0.0f && len2(h.point_bt - w.ray_source_bt) < min_hit_dist_sq_bt) continue;
+            if (!best.hit || h.t < best.t) {
+                best = h;
+                best_idx = i;
+                best_nr = o.demo_no_contact_response != 0;
+            }
+        }
+        if (best.hit && (!hit.hit || best.t < hit.t)) {
+            hit = best;
+            hit_world = false;
+            ground_car_idx = best_idx;
+            selected_no_response = best_nr;
+        }
+    }
     {
         RayHit bh;
         if (wheel_ray_vs_ball(w.ray_source_bt, w.wheel_dir_ws, real_ray_length, ball, tc.ball_radius,
@@ -315,8 +521,14 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
                 hit = bh;
                 ground_car_idx = -1;
                 hit_world = false;
+                selected_no_response = false;
             }
         }
+    }
+    if (selected_no_response) {
+        hit.hit = 0;
+        hit_world = false;
+        ground_car_idx = -1;
     }
     const V3 car_up = -w.wheel_dir_ws;
     if (hit.hit) {
@@ -717,6 +929,38 @@ RG_HDI void apply_boost(CarState& c, const CarControls& k, const TickConfig& tc,
 // ---- the vehicle update -------------------------------------------------------------------------------------------
 // reference PreTickCar (env_step.hpp:3115-3484) with PreTickVehicleDynamics (raycast_wheels_and_contact_prep.hpp:
 // 2618-2953), WheelRayPhase (:2074-2238) and CombineWheelContacts (:2240-2282).
+// The contact impulse denominator of a body at a point, inverse inertia applied column-wise (reference
+// BodyImpulseDenominatorBt with ApplyInverseBodyInertiaWorldBtColumnDot, host_validation_and_contact_debug.hpp:333-411).
+RG_HDI float car_impulse_denominator_bt(const CarState& c, const CarConfig& cfg, float mass, V3 p, V3 n) {
+    const V3 rel = p - c.pos_bt;
+    const V3 c0 = cross(rel, n);
+    V3 r0, r1, r2;
+    car_inv_inertia_world_bt(c, cfg, mass, r0, r1, r2);
+    const V3 ang{r0.x * c0.x + r1.x * c0.y + r2.x * c0.z, r0.y * c0.x + r1.y * c0.y + r2.y * c0.z,
+                 r0.z * c0.x + r1.z * c0.y + r2.z * c0.z};
+    return 1.0f / mass + dot(n, cross(ang, rel));
+}
+RG_HDI float car_car_wheel_pushback(const CarState& c, const CarConfig& cfg, const CarState& o, const CarConfig& ocfg,
+                                    float mass, V3 p, V3 n, float distance_bt, float dt) {
+    const V3 v1 = c.vel_bt + cross(c.ang_vel, p - c.pos_bt);
+    const V3 v2 = o.vel_bt + cross(o.ang_vel, p - o.pos_bt);
+    const float rel = dot(n, v1 - v2);
+    const float d0 = car_impulse_denominator_bt(c, cfg, mass, p, n);
+    const float d1 = car_impulse_denominator_bt(o, ocfg, mass, p, n);
+    if (dt <= 0.0f || d0 + d1 <= 0.0f) return 0.0f;
+    const float jac = 1.0f / (d0 + d1);
+    const float imp = (0.2f * -distance_bt / dt) * jac + -rel * jac;
+    return imp > 0.0f ? imp : 0.0f;
+}
+RG_HDI void car_impulse_at_point_bt(CarState& c, const CarConfig& cfg, float mass, V3 impulse, V3 rel) {
+    car_set_vel_bt(c, c.vel_bt + impulse * (1.0f / mass));
+    c.vel_touched_solve_stage = 1;
+    const V3 torque = cross(rel, impulse);
+    V3 r0, r1, r2;
+    car_inv_inertia_world_bt(c, cfg, mass, r0, r1, r2);
+    c.ang_vel = c.ang_vel + V3{dot(r0, torque), dot(r1, torque), dot(r2, torque)};
+}
+
 // Wheel rays that landed on the ball this tick, in the car's wheel order: each pushes the ball down along the hit
 // normal. Nothing else in a car's vehicle update reads the ball's velocity, so the pushes are recorded and applied
 // afterwards in the arena's car order, which keeps the reference's floating-point order (reference WheelRayPhase,
@@ -737,7 +981,8 @@ RG_HDI void apply_wheel_ball_pushes(BallState& ball, const WheelBallPushes& p, c
 }
 
 RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg, const TickConfig& tc,
-                           WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, WheelBallPushes& pushes) {
+                           WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, const WheelOthers& oth,
+                           WheelBallPushes& pushes) {
     pushes.count = 0;
     const float dt = tc.tick_dt;
     c.demo_no_contact_response = c.is_demoed ? 1 : 0;
@@ -787,10 +1032,30 @@ RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cf
             init_wheel(w, c, cfg, i, f, i < 2 ? front_bone : back_bone);
             w.suspension_force_scale = w.is_front_wheel ? front_scale : back_scale;
             w.extra_pushback = wr.extra_pushback[i];
-            wheel_ray_cast(c, w, ball, tc, mesh, min_hit_dist_sq);
+            wheel_ray_cast(c, w, ball, tc, mesh, min_hit_dist_sq, oth);
             if (w.is_in_contact) w.extra_pushback = 0.0f;
             if (w.is_in_contact_with_world) world_wheel_pushback(c, tc, w, f);
-            if (w.is_in_contact && !w.is_in_contact_with_world && w.ground_kind == kRayHitBall) {
+            if (w.is_in_contact && !w.is_in_contact_with_world && w.ground_kind == kRayHitCar && oth.cars &&
+                w.ground_car_idx >= 0 && w.ground_car_idx < oth.count && w.ground_car_idx != oth.self) {
+                // a wheel on another car pushes that car down (and back out when pressed in) at once (reference
+                // WheelRayPhase, :2196-2219; ResolveCarCarWheelPushbackMagnitudeBtInputs, ApplyImpulseAtPointBt-
+                // RoundtripBtInputs, host_validation_and_contact_debug.hpp:413-482)
+                CarState& o = oth.cars[w.ground_car_idx];
+                const CarConfig& ocfg = oth.cfgs[w.ground_car_idx];
+                const V3 n_bt = w.contact_normal_ws, cp_bt = w.contact_point_bt;
+                const float solver_dt = 1.0f / 60.0f;
+                const float thresh = (w.suspension_rest_length * kUuToBt + w.wheel_radius * kUuToBt) - 0.05f;
+                w.extra_pushback = 0.0f;
+                if (w.wheel_trace_len_bt < thresh)
+                    w.extra_pushback = car_car_wheel_pushback(c, cfg, o, ocfg, tc.car_mass, cp_bt, n_bt,
+                                                              w.wheel_trace_len_bt - thresh, solver_dt) /
+                                       4.0f;
+                if (w.extra_pushback > 0.0f) {
+                    const float full = w.extra_pushback * 4.0f;
+                    car_impulse_at_point_bt(o, ocfg, tc.car_mass, -n_bt * full, cp_bt - o.pos_bt);
+                }
+                car_impulse_at_point_bt(o, ocfg, tc.car_mass, -n_bt, cp_bt - o.pos_bt);
+            } else if (w.is_in_contact && !w.is_in_contact_with_world && w.ground_kind == kRayHitBall) {
                 // the ray pushes the ball down (reference WheelRayPhase, :2200-2207); the caller applies the push in
                 // the arena's car order (apply_wheel_ball_pushes)
                 pushes.point_bt[pushes.count] = w.contact_point_bt;
@@ -1025,7 +1290,10 @@ RG_HDI void car_world_prestep(CarState& c, const CarConfig& cfg, const WheelRunt
 RG_HDI void car_world_finish(CarState& c, const PreContactCar& pre, float sub_dt) {
     if (pre.is_demoed) return;
     if (c.just_respawned) return;
-    if (c.ext_force_impulse_bt_valid && !c.is_demoed) {
+    // A car demolished during this step's car pairs takes the reference's fallback (ComputeOfficialExternalForce-
+    // ImpulseBt from the same wheel record), which yields the impulses the prestep stored
+    // (ApplyDeferredVelocityDeltas, host_validation_and_contact_debug.hpp:986-1023).
+    if (c.ext_force_impulse_bt_valid) {
         car_set_vel_bt(c, c.vel_bt + c.ext_force_impulse_bt);
         c.ang_vel += c.ext_torque_impulse;
     }
