@@ -46,9 +46,10 @@ WORKLOADS = {
              "11k-tri arena, 8 ticks per launch",
     "balls": "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step",
 }
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel at each workload, from the ncu
-# captures summarised under profiles/ (None: not captured)
-TRAFFIC_PER_LAUNCH = {"balls": 16.01e6, "mixed": None}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per step, from the ncu captures summarised under profiles/:
+# balls, one tick_kernel launch of 8 ticks at 16,384 arenas; mixed, arena_finish + car_vehicle per tick at 4,096
+# arenas times 8 ticks, scaled by 4 to 16,384 arenas (profiles/tick_kernels_mixed_car_arenas.md)
+TRAFFIC_PER_LAUNCH = {"balls": 16.01e6, "mixed": 1.72e9}
 
 
 def peaks():
@@ -277,11 +278,13 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"arena shards x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_kind, "traffic": TRAFFIC_PER_LAUNCH[args.workload],
-                     "note": "algorithmic state bytes per launch / launch time; the tick is FP32-issue / latency "
-                             "bound (data-dependent branches, dependent loads), not HBM bound"},
+                     "note": "per step (mixed: 8 ticks x 4 launches): algorithmic state bytes / step time; the tick is "
+                             "latency bound (one thread per arena, data-dependent branches, dependent loads), not HBM "
+                             "bound"},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        # mixed: three kernels per tick (arena begin, per-car vehicle update, arena finish); balls: one per step
-        "gpu_launches": args.steps * TICKS_PER_STEP * 3 if mixed else args.steps,
+        # mixed: four kernels per tick (arena begin, per-car tick start, per-car vehicle update, arena finish);
+        # balls: one per step
+        "gpu_launches": args.steps * TICKS_PER_STEP * 4 if mixed else args.steps,
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,7 +357,12 @@ def main():
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--arenas", type=int, default=ENVS, help="arenas per GPU (smaller cases for profiling)")
     args = ap.parse_args()
+    if args.arenas != ENVS:
+        globals()["ENVS"] = args.arenas
+        for k in WORKLOADS:
+            WORKLOADS[k] = WORKLOADS[k].replace("16384 arenas", f"{args.arenas} arenas")
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -5,8 +5,8 @@ boost pads of every arena.
 Scope of this build: cars in the air and on their wheels (controls, jumps, dodges, boost, air control, suspension,
 tyre friction, sticky force, pads), the car body's contacts with the arena mesh (landings on the roof or a side,
 wall hits) with the broadphase manifold list that orders the solver, and car-ball contacts (the retained car-ball
-manifold, the two-body rows in the unified solve, the ball-hit records and the game's extra hit impulse). Contacts
-between two cars are not built, so the kickoff scenarios run one car per arena.
+manifold, the two-body rows in the unified solve, the ball-hit records and the game's extra hit impulse). These
+scenarios run one car per arena; arenas with several cars are covered by test_car_car_parity.py.
 """
 import numpy as np
 import pytest
