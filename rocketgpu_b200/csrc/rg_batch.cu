@@ -390,14 +390,15 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
 }
 
 // The step order (reference set_env_car_count rebuilds its step order, src/rocketgpu.cpp:2920-2932): arenas stably
-// sorted by car count, and the active car slots of those arenas in that order. The host copies stay in the batch
+// sorted by car count, largest first (their warps run longest, so they start first and the short ones fill in behind
+// them), and the active car slots of those arenas in that order. The host copies stay in the batch
 // until the caller's stream has finished the upload (set_env_car_count synchronises it).
 void rebuild_step_order(rg_batch* b, cudaStream_t s) {
     std::vector<int32_t>& order = b->host_arena_order;
     order.resize(b->env_count);
     for (int32_t e = 0; e < b->env_count; ++e) order[e] = e;
     std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t x, int32_t y) { return b->host_car_count[x] < b->host_car_count[y]; });
+                     [&](int32_t x, int32_t y) { return b->host_car_count[x] > b->host_car_count[y]; });
     std::vector<int32_t>& cars = b->host_active_cars;
     cars.clear();
     for (int32_t e : order)
