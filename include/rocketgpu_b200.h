@@ -172,7 +172,7 @@ typedef struct rg_env_command {
  * MutatorConfig fields the tick reads, rocketgpu.h:708-840). Zero-initialise, then call rg_sim_config_default. */
 typedef struct rg_sim_config {
     int32_t env_count;
-    int32_t max_cars_per_env;       /* 0..8 */
+    int32_t max_cars_per_env;       /* 0..6 (the reference allows 8; 7- and 8-car arenas are refused here) */
     float tick_dt;                   /* 1/120 */
     uint8_t enable_boost_pads, enable_car_car_collisions, enable_demos, enable_scoring;
     uint64_t respawn_rng_seed;
@@ -180,6 +180,8 @@ typedef struct rg_sim_config {
     float gravity_z, ball_radius, ball_mass, car_mass, ball_drag, ball_friction, ball_restitution, ball_max_speed,
         ball_max_ang_speed, car_max_speed, car_max_ang_speed, arena_friction, arena_restitution,
         goal_base_threshold_y;
+    /* Must be 0: kickoff settling (reference MutatorConfig::kickoff_settled, default 1 there) is not built, so
+     * rg_sim_config_default sets 0 and rg_batch_create refuses 1 (status 2). */
     uint8_t kickoff_settled;
     uint8_t reserved[7];
 } rg_sim_config;
@@ -245,8 +247,8 @@ RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, vo
 /* BatchSim::reset_to_kickoff (rocketgpu.h:1070; src/rocketgpu.cpp:2085-2132, ResetEnvToKickoff arena_ball.hpp:
  * 3054-3085): every arena to kickoff, the spot order drawn from `seed` (0: from the arena's reset count). Car
  * contact state and the ball's manifolds are cleared; wheel records are kept, as the reference keeps them.
- * rg_batch_create ends with reset_to_kickoff(0). Kickoff-settle copies (SimConfig.kickoff_settled) are not built:
- * the reset is the reference's with kickoff_settled = 0. */
+ * rg_batch_create ends with reset_to_kickoff(0). The reset is the reference's with kickoff_settled = 0 (the only
+ * value rg_batch_create accepts). */
 RG_API int rg_batch_reset_to_kickoff(rg_batch* b, uint64_t seed, void* stream);
 /* BatchSim::upload_controls (rocketgpu.h:1032): the controls rg_batch_step holds for every tick. */
 RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream);
@@ -260,7 +262,38 @@ RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream);
 RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls* device_controls, int32_t ticks,
                                               int32_t control_stride, void* stream);
 
-/* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
+/* BatchSim::apply_env_commands (rocketgpu.h:1066; src/rocketgpu.cpp:2136-2218; ApplyEnvCommand env_step.hpp:
+ * 5672-5758): command i for env i, applied between steps. reset_to_kickoff resets the env to kickoff (with
+ * reset_scoreboard = 0: scores and tick kept and, with no seed, the match's next kickoff order; keep_boost_pads keeps
+ * the pads); reset_scoreboard / reset_tick_count then clear the score / tick (only together with a reset, as in the
+ * reference); new_round_bodies takes every body out of the broadphase as the game does after a goal. The host array
+ * is borrowed for the call (the call synchronises the stream). kickoff_countdown_ticks != 0 (the game's countdown
+ * spawn) is not built: such a command is refused (invalid_argument) and nothing is applied. */
+RG_API int rg_batch_apply_env_commands(rg_batch* b, const rg_env_command* host_commands, size_t count, void* stream);
+/* BatchSim::apply_env_commands_device (rocketgpu.h:1067): as above with a device array, asynchronous. A command with
+ * kickoff_countdown_ticks != 0 leaves its env unchanged and the next rg_batch_synchronize reports invalid_argument. */
+RG_API int rg_batch_apply_env_commands_device(rg_batch* b, const rg_env_command* device_commands, size_t count,
+                                              void* stream);
+/* BatchSim::step_with_device_commands (rocketgpu.h:1077; src/rocketgpu.cpp:2554-2575): as
+ * rg_batch_step_with_device_controls, and at the start of tick t env e first applies
+ * device_commands[t * command_stride + e] (StepEnvPreTickEnv, env_step.hpp:6701-6749); command_stride must be at
+ * least env_count. Refused commands are reported as for rg_batch_apply_env_commands_device. */
+RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls* device_controls,
+                                              int32_t control_stride, const rg_env_command* device_commands,
+                                              int32_t command_stride, int32_t ticks, void* stream);
+/* Episode resets for training loops, on the device. No counterpart in BatchSim: the reference's own benchmark makes
+ * the same decisions on the host between steps (tools/bench_cpp.cpp:104-112). Writes device_commands[e] for every
+ * env: a fresh-episode reset (reset_to_kickoff = reset_scoreboard = reset_tick_count = 1, kickoff_seed 0) when the
+ * env's score is non-zero (a goal this episode) or no car has touched the ball for no_touch_ticks ticks, else an
+ * all-zero command; pass the array to the next rg_batch_step_with_device_commands (stride env_count, first tick).
+ * Touches are seen through each car's latest_touch_tick changing between calls. init != 0 starts the episode clocks
+ * instead (writes all-zero commands): each env's clock starts at an age in [0, no_touch_ticks) drawn from
+ * stagger_seed (0: age 0), so resets spread out over the ticks. The batch keeps the clocks (16 bytes per env). */
+RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64_t stagger_seed, int32_t init,
+                                     rg_env_command* device_commands, void* stream);
+
+/* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch, and a device env
+ * command that was refused (invalid_argument). */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
 
 /* The arena tables rg_batch_create builds from a layout, for inspection: per triangle (caller order) 16 floats

@@ -1,7 +1,7 @@
 """ctypes binding of include/rocketgpu_b200.h (the in-tree CUDA library rocketgpu_b200/_lib/librocketgpu_b200.so).
 
-This is the binding a ctypes/cffi user of the C ABI writes; the pybind / Rust shims of the reference would bind the
-same symbols.
+This is the binding a ctypes/cffi user of the C ABI writes; a pybind11 module or a Rust FFI crate binds the same
+symbols.
 """
 from __future__ import annotations
 
@@ -22,7 +22,8 @@ EXPORTS = [
     "rg_default_car_state", "rg_default_car_config", "rg_batch_upload_car_states", "rg_batch_download_car_states",
     "rg_batch_pad_capacity", "rg_batch_upload_pad_states", "rg_batch_download_pad_states", "rg_batch_set_car_configs",
     "rg_batch_upload_controls", "rg_batch_step_with_device_controls", "rg_batch_set_teams",
-    "rg_batch_reset_to_kickoff",
+    "rg_batch_reset_to_kickoff", "rg_batch_apply_env_commands", "rg_batch_apply_env_commands_device",
+    "rg_batch_step_with_device_commands", "rg_batch_episode_commands",
 ]
 
 
@@ -98,5 +99,9 @@ def lib():
         L.rg_batch_pad_capacity.restype = i64
         L.rg_batch_step_with_device_controls.argtypes = [vp, vp, i32, i32, vp]
         L.rg_batch_reset_to_kickoff.argtypes = [vp, ctypes.c_uint64, vp]
+        L.rg_batch_apply_env_commands.argtypes = [vp, vp, sz, vp]
+        L.rg_batch_apply_env_commands_device.argtypes = [vp, vp, sz, vp]
+        L.rg_batch_step_with_device_commands.argtypes = [vp, vp, i32, vp, i32, i32, vp]
+        L.rg_batch_episode_commands.argtypes = [vp, i32, ctypes.c_uint64, i32, vp, vp]
         _lib = L
     return _lib

@@ -15,7 +15,14 @@ import numpy as np
 
 from . import abi
 
-CAR_BYTES, BALL_BYTES, ENV_BYTES, PAD_BYTES, CONTROLS_BYTES, CAR_CONFIG_BYTES = 880, 288, 44, 16, 24, 120
+CAR_BYTES, BALL_BYTES, ENV_BYTES, PAD_BYTES, CONTROLS_BYTES, CAR_CONFIG_BYTES, ENV_COMMAND_BYTES = \
+    880, 288, 44, 16, 24, 120, 16
+
+# rg_env_command / the reference's EnvCommand (rocketgpu.h:683-706) as a numpy record
+ENV_COMMAND_DTYPE = np.dtype([("reset_to_kickoff", "u1"), ("reset_scoreboard", "u1"), ("reset_tick_count", "u1"),
+                              ("kickoff_seed_mode", "u1"), ("new_round_bodies", "u1"), ("keep_boost_pads", "u1"),
+                              ("kickoff_countdown_ticks", "<u2"), ("kickoff_seed", "<u8")])
+assert ENV_COMMAND_DTYPE.itemsize == ENV_COMMAND_BYTES
 
 
 def _check(rc: int):
@@ -150,6 +157,25 @@ class BatchSim:
         """`device_controls` is a device pointer to rg_car_controls rows (e.g. a torch uint8 tensor's data_ptr())."""
         _check(abi.lib().rg_batch_step_with_device_controls(self._h, ctypes.c_void_p(device_controls), ticks,
                                                             control_stride, stream))
+
+    def apply_env_commands(self, commands: np.ndarray, stream: int = 0):
+        """`commands`: ENV_COMMAND_DTYPE records (or uint8 rows of 16 bytes), one per env from env 0."""
+        c = np.ascontiguousarray(commands).view(np.uint8).reshape(-1, ENV_COMMAND_BYTES)
+        _check(abi.lib().rg_batch_apply_env_commands(self._h, _ptr(c), len(c), stream))
+
+    def apply_env_commands_device(self, device_commands: int, count: int, stream: int = 0):
+        _check(abi.lib().rg_batch_apply_env_commands_device(self._h, ctypes.c_void_p(device_commands), count, stream))
+
+    def step_with_device_commands(self, device_controls: int, control_stride: int, device_commands: int,
+                                  command_stride: int, ticks: int, stream: int = 0):
+        _check(abi.lib().rg_batch_step_with_device_commands(self._h, ctypes.c_void_p(device_controls), control_stride,
+                                                            ctypes.c_void_p(device_commands), command_stride, ticks,
+                                                            stream))
+
+    def episode_commands(self, no_touch_ticks: int, device_commands: int, stagger_seed: int = 0, init: bool = False,
+                         stream: int = 0):
+        _check(abi.lib().rg_batch_episode_commands(self._h, no_touch_ticks, stagger_seed, int(init),
+                                                   ctypes.c_void_p(device_commands), stream))
 
     def step(self, ticks: int = 1, stream: int = 0):
         _check(abi.lib().rg_batch_step(self._h, ticks, stream))

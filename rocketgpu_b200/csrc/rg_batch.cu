@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -107,6 +108,10 @@ struct rg_batch {
     std::vector<int32_t> host_arena_order, host_active_cars;
     int launch_threads = 32;
     int pair_slots = 0;
+    DeviceArray<rg::EnvCommand> command_scratch;  // per arena: the host commands of rg_batch_apply_env_commands
+    DeviceArray<uint32_t> device_status;          // bit 0: a device command asked for something this build refuses
+    DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
+    DeviceArray<uint64_t> episode_seen;           // per car slot: latest_touch_tick at the previous episode check
 };
 
 namespace {
@@ -216,6 +221,10 @@ struct CarTickArgs {
     const int32_t* arena_order;
     const int32_t* active_cars;
     int32_t active_car_count;
+    const rg::EnvCommand* commands;  // step_with_device_commands: tick t's command for arena e at t * stride + e
+    int32_t command_stride;
+    rg::CarControls* reset_controls;  // the batch's held controls, cleared by a kickoff reset
+    uint32_t* status;
 };
 
 __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e, int t) {
@@ -235,11 +244,53 @@ __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e,
     return A;
 }
 
-// Tick part 1, one thread per arena in step order: vehicle order, the ball's tick start, pad timers.
+__device__ __forceinline__ rg::ArenaContactState arena_contact_state(const CarTickArgs& a, int e) {
+    rg::ArenaContactState cs;
+    cs.ball_world = a.base.ball_world + e;
+    cs.bp = a.broadphase + e;
+    cs.car_world = a.car_world + static_cast<size_t>(e) * a.max_cars;
+    cs.ball_car = a.ball_car + static_cast<size_t>(e) * a.max_cars;
+    cs.pairs = a.pair_slots ? a.pairs + static_cast<size_t>(e) * a.pair_slots : nullptr;
+    cs.pair_slots = a.pair_slots;
+    return cs;
+}
+
+// A command this build does not run (the game's countdown spawn): flag it for the host instead of resetting
+// differently from the reference; the arena is left as it was.
+__device__ __forceinline__ bool command_refused(const rg::EnvCommand& c, uint32_t* status) {
+    if (c.reset_to_kickoff && c.kickoff_countdown_ticks != 0) {
+        atomicOr(status, 1u);
+        return true;
+    }
+    return false;
+}
+
+// Env commands between steps, one thread per arena (reference LaunchApplyEnvCommands / apply_env_commands_host,
+// src/rocketgpu.cpp:2136-2218).
+__global__ void apply_commands_kernel(CarTickArgs a, const rg::EnvCommand* cmds, int n, rg::CarControls* controls,
+                                      uint32_t* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const rg::EnvCommand c = cmds[e];
+    if (!rg::env_command_active(c) || command_refused(c, status)) return;
+    rg::ArenaCars A = arena_cars(a, e, 0);
+    rg::apply_env_command(c, e, a.base.envs[e], a.base.balls[e], arena_contact_state(a, e), A,
+                          controls + static_cast<size_t>(e) * a.max_cars, a.pad_layout, a.base.tc);
+}
+
+// Tick part 1, one thread per arena in step order: this tick's env command (step_with_device_commands), vehicle
+// order, the ball's tick start, pad timers.
 __global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
+    if (a.commands) {
+        const rg::EnvCommand c = a.commands[static_cast<size_t>(t) * static_cast<size_t>(a.command_stride) + e];
+        if (rg::env_command_active(c) && !command_refused(c, a.status))
+            rg::apply_env_command(c, e, a.base.envs[e], a.base.balls[e], arena_contact_state(a, e),
+                                  arena_cars(a, e, t), a.reset_controls + static_cast<size_t>(e) * a.max_cars,
+                                  a.pad_layout, a.base.tc);
+    }
     rg::BallState b = a.base.balls[e];
     rg::EnvState env = a.base.envs[e];
     rg::arena_tick_begin(env, b, arena_cars(a, e, t), a.base.tc, a.pad_layout, a.snaps[e]);
@@ -273,11 +324,16 @@ __global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
     const int idx = a.active_cars[k];
     const int e = idx / a.max_cars;
     const int base = e * a.max_cars;
-    if (rg::arena_wheel_reach_near(a.cars + base, a.car_cfgs + base, a.base.env_car_count[e])) return;
+    const int count = a.base.env_car_count[e];
+    if (rg::arena_wheel_reach_near(a.cars + base, a.car_cfgs + base, count)) return;
     const rg::CarControls& ctrl =
         a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+    const uint32_t excluded =
+        a.cars[idx].is_demoed ? 0u
+                              : rg::wheel_ray_excluded_bodies(a.cars[idx], a.car_cfgs[idx], a.broadphase + e, idx - base,
+                                                              count);
     rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], a.base.mesh,
-                       rg::WheelOthers{nullptr, nullptr, 0, -1}, a.records[idx].pushes);
+                       rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes);
 }
 
 // Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
@@ -326,13 +382,25 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     a.arena_order = b->arena_order.ptr;
     a.active_cars = b->active_cars.ptr;
     a.active_car_count = b->active_car_count;
+    a.commands = nullptr;
+    a.command_stride = 0;
+    a.reset_controls = b->controls.ptr;
+    a.status = b->device_status.ptr;
     return a;
 }
 
 // Arenas with cars: four launches per tick (arena begin, per-car tick start, per-car vehicle update, arena finish).
-void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s) {
+void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s,
+                     const rg::EnvCommand* commands = nullptr, int command_stride = 0) {
     if (b->env_count == 0) return;
-    const CarTickArgs a = car_tick_args(b, controls, stride);
+    CarTickArgs a = car_tick_args(b, controls, stride);
+    a.commands = commands;
+    a.command_stride = command_stride;
+    if (commands) {
+        // a reset may give pads their initial state and put cars on the field: pads take part from here on
+        a.pads = b->pads.ptr;
+        b->pads_live = true;
+    }
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
     const int car_blocks = (b->active_car_count + 63) / 64;
@@ -340,7 +408,9 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
         arena_begin_kernel<<<blocks, threads, 0, s>>>(a, t);
         if (car_blocks) car_pre_kernel<<<car_blocks, 64, 0, s>>>(a, t);
         if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s>>>(a, t);
-        arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, t + 1 == ticks ? 1 : 0);
+        // report fields after the last tick, and after every tick of a command stream (reference StepEnvGeneric,
+        // env_step.hpp:7174: report_fields = last tick || has_commands)
+        arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, (t + 1 == ticks || commands) ? 1 : 0);
     }
     check(cudaGetLastError(), "car tick launch");
 }
@@ -362,6 +432,54 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
                              a.car_cfgs + car_base, controls + car_base,
                              a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
                              teams + car_base, a.base.env_car_count[e], a.max_cars, a.base.tc);
+}
+
+// Episode resets for training loops (no counterpart in BatchSim; the reference's benchmark makes these decisions on
+// the host, tools/bench_cpp.cpp:104-112): an arena whose ball was scored (every reset clears the scoreboard, so a
+// non-zero score is a goal this episode) or that no car touched for `no_touch_ticks` ticks gets a fresh-episode reset
+// for the next step. Touches are noticed through each car's latest_touch_tick changing since the previous check, so a
+// value left over from an earlier episode never counts. `stagger` != 0 starts every arena's clock at a seeded age in
+// [0, no_touch_ticks) so that resets spread over the ticks instead of coming together.
+__device__ __forceinline__ uint64_t episode_hash(uint64_t x) {
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+__global__ void episode_commands_kernel(const rg::EnvState* envs, const rg::CarState* cars, const int32_t* counts,
+                                        int64_t* touch, uint64_t* seen, rg::EnvCommand* out, int n, int max_cars,
+                                        int32_t no_touch_ticks, uint64_t seed, int init) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const rg::EnvState& env = envs[e];
+    const int count = counts[e];
+    const size_t base = static_cast<size_t>(e) * max_cars;
+    rg::EnvCommand c;
+    memset(&c, 0, sizeof(c));
+    if (init) {
+        for (int i = 0; i < max_cars; ++i) seen[base + i] = cars[base + i].latest_touch_tick;
+        touch[e] = static_cast<int64_t>(env.tick) -
+                   (seed ? static_cast<int64_t>(episode_hash(seed ^ static_cast<uint64_t>(e)) %
+                                                static_cast<uint64_t>(no_touch_ticks))
+                         : 0);
+        out[e] = c;
+        return;
+    }
+    int64_t last = touch[e];
+    for (int i = 0; i < count; ++i) {
+        const uint64_t v = cars[base + i].latest_touch_tick;
+        if (v != seen[base + i]) {
+            seen[base + i] = v;
+            if (v != ~0ull && static_cast<int64_t>(v) > last) last = static_cast<int64_t>(v);
+        }
+    }
+    const bool scored = (env.blue_score | env.orange_score) != 0;
+    if (scored || static_cast<int64_t>(env.tick) - last >= no_touch_ticks) {
+        c.reset_to_kickoff = c.reset_scoreboard = c.reset_tick_count = 1;
+        last = 0;
+    }
+    touch[e] = last;
+    out[e] = c;
 }
 
 void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
@@ -479,7 +597,8 @@ RG_API void rg_sim_config_default(rg_sim_config* c) {
     c->arena_friction = 0.30f;
     c->arena_restitution = 0.30f;
     c->goal_base_threshold_y = 5124.2373046875f;
-    c->kickoff_settled = 1;
+    // the reference defaults to 1 (rocketgpu.h:831); this build has no kickoff settling and refuses 1
+    c->kickoff_settled = 0;
 }
 
 RG_API void rg_default_ball_state(rg_ball_state* o) {
@@ -560,8 +679,15 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
     return guard([&] {
         if (!cfg || !layout || !out) throw std::invalid_argument("null argument");
         if (cfg->env_count <= 0) throw std::invalid_argument("env_count must be positive");
-        if (cfg->max_cars_per_env < 0 || cfg->max_cars_per_env > 8)
-            throw std::invalid_argument("max_cars_per_env must be in [0, 8]");
+        // The car-car pair rows are sized for the 15 pairs of six cars (rg_car_car.cuh kMaxPairRows); 7- and 8-car
+        // arenas would need more, so they are refused rather than run with rows dropped.
+        if (cfg->max_cars_per_env < 0 || cfg->max_cars_per_env > 6)
+            throw std::invalid_argument("max_cars_per_env must be in [0, 6]");
+        // Kickoff settling (the reference's MutatorConfig::kickoff_settled, src/rocketgpu.cpp:1538-1603: kickoffs
+        // that start from the state the game's countdown leaves) is not built: refuse it instead of resetting
+        // differently from the reference.
+        if (cfg->kickoff_settled != 0)
+            throw std::invalid_argument("kickoff_settled = 1 is not supported by this build; set it to 0");
         if (!(cfg->tick_dt > 0.0f)) throw std::invalid_argument("tick_dt must be positive");
         std::unique_ptr<rg_batch> b(new rg_batch);
         b->device = device;
@@ -622,6 +748,13 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
                   "car-car manifolds");
         b->car_records.alloc(cap);
         b->arena_snaps.alloc(b->env_count);
+        b->command_scratch.alloc(b->env_count);
+        b->device_status.alloc(1);
+        check(cudaMemset(b->device_status.ptr, 0, sizeof(uint32_t)), "device status");
+        b->episode_touch.alloc(b->env_count);
+        check(cudaMemset(b->episode_touch.ptr, 0, b->env_count * sizeof(int64_t)), "episode state");
+        b->episode_seen.alloc(cap);
+        if (cap) check(cudaMemset(b->episode_seen.ptr, 0xff, cap * sizeof(uint64_t)), "episode state");
         b->arena_order.alloc(b->env_count);
         b->active_cars.alloc(cap);
         rebuild_step_order(b.get(), nullptr);
@@ -875,11 +1008,96 @@ RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls
     });
 }
 
+RG_API int rg_batch_apply_env_commands(rg_batch* b, const rg_env_command* host, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || !host) throw std::invalid_argument("host_commands must not be null");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("apply_env_commands count exceeds env_count");
+        size_t active = 0;
+        for (size_t i = 0; i < count; ++i) {
+            const rg_env_command& c = host[i];
+            if (c.reset_to_kickoff && c.kickoff_countdown_ticks != 0)
+                throw std::invalid_argument("kickoff_countdown_ticks != 0 is not supported (the game's countdown spawn "
+                                            "is not built)");
+            active += (c.reset_to_kickoff | c.reset_scoreboard | c.reset_tick_count | c.new_round_bodies) != 0;
+        }
+        if (active == 0) return;
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(b->command_scratch.ptr, host, count * sizeof(rg_env_command), cudaMemcpyHostToDevice, s),
+              "apply_env_commands upload");
+        CarTickArgs a = car_tick_args(b, nullptr, 0);
+        a.pads = b->pads.ptr;
+        apply_commands_kernel<<<(static_cast<int>(count) + 63) / 64, 64, 0, s>>>(
+            a, b->command_scratch.ptr, static_cast<int>(count), b->controls.ptr, b->device_status.ptr);
+        check(cudaGetLastError(), "apply_commands_kernel launch");
+        // the host array is borrowed for the call only
+        check(cudaStreamSynchronize(s), "apply_env_commands sync");
+    });
+}
+
+RG_API int rg_batch_apply_env_commands_device(rg_batch* b, const rg_env_command* device_commands, size_t count,
+                                              void* stream) {
+    return guard([&] {
+        if (!b || !device_commands) throw std::invalid_argument("device_commands must not be null");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("apply_env_commands_device count exceeds env_count");
+        if (count == 0) return;
+        DeviceGuard dg(b->device);
+        CarTickArgs a = car_tick_args(b, nullptr, 0);
+        a.pads = b->pads.ptr;
+        apply_commands_kernel<<<(static_cast<int>(count) + 63) / 64, 64, 0, static_cast<cudaStream_t>(stream)>>>(
+            a, reinterpret_cast<const rg::EnvCommand*>(device_commands), static_cast<int>(count), b->controls.ptr,
+            b->device_status.ptr);
+        check(cudaGetLastError(), "apply_commands_kernel launch");
+    });
+}
+
+RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls* device_controls,
+                                              int32_t control_stride, const rg_env_command* device_commands,
+                                              int32_t command_stride, int32_t ticks, void* stream) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        if (ticks <= 0) return;
+        if (!device_controls) throw std::invalid_argument("device_controls_by_tick must not be null");
+        if (!device_commands) throw std::invalid_argument("device_env_commands_by_tick must not be null");
+        if (control_stride < 0 || (control_stride != 0 && static_cast<int64_t>(control_stride) < rg_batch_car_capacity(b)))
+            throw std::invalid_argument("control_stride must be zero or at least the total car capacity");
+        if (command_stride < b->env_count) throw std::invalid_argument("env_command_stride must be at least env_count");
+        DeviceGuard dg(b->device);
+        launch_car_tick(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
+                        static_cast<cudaStream_t>(stream), reinterpret_cast<const rg::EnvCommand*>(device_commands),
+                        command_stride);
+    });
+}
+
+RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64_t stagger_seed, int32_t init,
+                                     rg_env_command* device_commands, void* stream) {
+    return guard([&] {
+        if (!b || !device_commands) throw std::invalid_argument("null argument");
+        if (no_touch_ticks <= 0) throw std::invalid_argument("no_touch_ticks must be positive");
+        DeviceGuard dg(b->device);
+        episode_commands_kernel<<<(b->env_count + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+            b->envs.ptr, b->cars.ptr, b->env_car_count.ptr, b->episode_touch.ptr, b->episode_seen.ptr,
+            reinterpret_cast<rg::EnvCommand*>(device_commands), b->env_count, b->max_cars, no_touch_ticks,
+            stagger_seed, init);
+        check(cudaGetLastError(), "episode_commands_kernel launch");
+    });
+}
+
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
     return guard([&] {
         if (!b) throw std::invalid_argument("null argument");
         DeviceGuard dg(b->device);
         check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
+        uint32_t status = 0;
+        check(cudaMemcpy(&status, b->device_status.ptr, sizeof(status), cudaMemcpyDeviceToHost), "device status");
+        if (status) {
+            check(cudaMemset(b->device_status.ptr, 0, sizeof(status)), "device status");
+            throw std::invalid_argument(
+                "a device env command asked for kickoff_countdown_ticks != 0 (the game's countdown spawn is not "
+                "built); those arenas were left unchanged");
+        }
     });
 }
 
@@ -937,18 +1155,22 @@ constexpr int kStaticScratchEnvs = 4096;
 static __device__ __align__(256) rg::BallWorldScratch g_static_ball_world[kStaticScratchEnvs];
 
 constexpr int kMaxDevices = 64;
-void* g_static_scratch_addr[kMaxDevices] = {};
+struct StaticScratchSlot {
+    std::once_flag once;
+    void* addr = nullptr;
+    cudaError_t status = cudaSuccess;
+};
+StaticScratchSlot g_static_scratch[kMaxDevices];
 
 // Device address of g_static_ball_world on the current device. In host code the symbol's name stands for a host-side
-// shadow, not the device array, so the address comes from cudaGetSymbolAddress, once per device.
+// shadow, not the device array, so the address comes from cudaGetSymbolAddress, once per device; the once_flag makes a
+// first call from several host threads at the same time look it up once and all see the result.
 rg::BallWorldScratch* static_scratch_address(int device) {
     if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device index out of range");
-    if (g_static_scratch_addr[device] == nullptr) {
-        void* p = nullptr;
-        check(cudaGetSymbolAddress(&p, g_static_ball_world), "cudaGetSymbolAddress(static scratch)");
-        g_static_scratch_addr[device] = p;
-    }
-    return static_cast<rg::BallWorldScratch*>(g_static_scratch_addr[device]);
+    StaticScratchSlot& slot = g_static_scratch[device];
+    std::call_once(slot.once, [&] { slot.status = cudaGetSymbolAddress(&slot.addr, g_static_ball_world); });
+    check(slot.status, "cudaGetSymbolAddress(static scratch)");
+    return static_cast<rg::BallWorldScratch*>(slot.addr);
 }
 }  // namespace
 

@@ -55,6 +55,11 @@ struct alignas(16) Broadphase {
     uint32_t manifolds[kBpMaxEntries];
     uint32_t predictive[kBpBodies];
     uint32_t pad1[3];
+    // each body's swept AABB as the last sweep saw it (Bullet units: min xyz, max xyz) and which entries hold one;
+    // suspension rays skip bodies whose box misses them (reference sap_body_aabb, arena_geometry.hpp:712-721)
+    float body_aabb[kBpBodies][6];
+    uint16_t body_aabb_valid;
+    uint16_t pad2[7];
 };
 
 // A body's broadphase proxy for this tick (reference BulletBroadphaseProxy).
@@ -336,6 +341,7 @@ struct Sweep {
         h.free_[h.free_count++] = static_cast<uint8_t>(handle);
         h.handle_count = static_cast<uint8_t>(h.handle_count - 1);
         h.body_handle[body] = 0;
+        h.body_aabb_valid = static_cast<uint16_t>(h.body_aabb_valid & ~(1u << body));
         for (int i = 0; i < h.obj_count; ++i) {
             if (h.obj[i] == body) {
                 h.obj[i] = h.obj[--h.obj_count];
@@ -445,6 +451,11 @@ struct Sweep {
             if (!p.valid || handle == 0) continue;
             const float lo[3] = {p.aabb_min.x, p.aabb_min.y, p.aabb_min.z};
             const float hi[3] = {p.aabb_max.x, p.aabb_max.y, p.aabb_max.z};
+            for (int a = 0; a < 3; ++a) {
+                h.body_aabb[body][a] = lo[a];
+                h.body_aabb[body][a + 3] = hi[a];
+            }
+            h.body_aabb_valid = static_cast<uint16_t>(h.body_aabb_valid | (1u << body));
             for (int axis = 0; axis < 3; ++axis) {
                 const uint16_t qmin = sweep_quantize(lo[axis], 0), qmax = sweep_quantize(hi[axis], 1);
                 const int emin = h.min_edge[handle][axis], emax = h.max_edge[handle][axis];

@@ -171,12 +171,54 @@ RG_HDI void reset_kickoff_ball(BallState& b) {
     b.sleeping = 1;
 }
 
-// The whole arena. `teams` are the arena's max_cars slot teams (0 blue, 1 orange); `scratch` is its persistent
-// contact state, cleared as the reference clears its solver scratch.
+// reference KickoffSpotPreferred / PreferKickoffSpotForShortTeam (arena_ball.hpp:2632-2653): a team with fewer cars
+// than the other also gets the best of the spots a full team would take (nearest the ball, then the left diagonal,
+// then the farther back).
+RG_HDI bool kickoff_spot_preferred(SpawnPos a, SpawnPos b) {
+    const float da = a.x * a.x + a.y * a.y;
+    const float db = b.x * b.x + b.y * b.y;
+    if (da != db) return da < db;
+    const bool left_a = a.x * a.y < 0.0f;
+    const bool left_b = b.x * b.y < 0.0f;
+    if (left_a != left_b) return left_a;
+    return (a.y < 0.0f ? -a.y : a.y) > (b.y < 0.0f ? -b.y : b.y);
+}
+RG_HDI void prefer_kickoff_spot_for_short_team(int* order, int team_count) {
+    constexpr int kMaxTeamSize = 4;
+    if (team_count <= 0 || team_count >= kMaxTeamSize) return;
+    int best = 0;
+    for (int i = 1; i < kMaxTeamSize; ++i)
+        if (kickoff_spot_preferred(soccar_kickoff_spawn(order[i]), soccar_kickoff_spawn(order[best]))) best = i;
+    if (best < team_count) return;
+    const int spot = order[best];
+    order[best] = order[team_count - 1];
+    order[team_count - 1] = spot;
+}
+
+// How a kickoff reset treats the match (the EnvCommand fields of the reference's ResetEnvToKickoff call,
+// env_step.hpp:5735-5752). The defaults are BatchSim::reset_to_kickoff's: a new match.
+struct KickoffReset {
+    bool preserve_score = false;  // keep scores, tick and last scorer; with seed 0, the match's next kickoff
+    uint8_t seed_mode = 0;        // 0: spot order from the seed (0: from the reset count); 2: as 0 with seed 0;
+                                  // 3: no shuffle, a team's nth car takes kickoff spot n
+    bool keep_pads = false;       // keep the pads and their timers
+};
+
+// The car slot visited k-th under `env`'s visit order (reference CarVisitSlot, rocketgpu.h:575-581).
+RG_HD int reset_visit_slot(const EnvState& env, int k, int count) {
+    if (env.car_visit_order_mode == 1 || env.car_visit_order_mode == 3)
+        return static_cast<int>((env.car_visit_order_packed >> (4 * k)) & 0xFu);
+    return env.car_visit_order_mode == 2 ? count - 1 - k : k;
+}
+
+// The whole arena (reference ResetEnvToKickoffState + ResetKickoffBall + ResetBoostPads + ResetKickoffCar,
+// arena_ball.hpp:2846-3085, with no platform respawn RNG, no settled-kickoff copy and no countdown). `teams` are the
+// arena's max_cars slot teams (0 blue, 1 orange); `scratch` is its persistent ball contact state, cleared as the
+// reference clears its solver scratch.
 RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, BallState& ball, BallWorldScratch& scratch,
                                  CarState* cars, const CarConfig* cfgs, CarControls* controls, PadState* pads,
                                  const PadLayout& L, const uint8_t* teams, int count, int max_cars,
-                                 const TickConfig& tc) {
+                                 const TickConfig& tc, const KickoffReset& how = KickoffReset{}) {
     memset(&scratch, 0, sizeof(scratch));
     const EnvState saved = env;
     EnvState next;
@@ -190,7 +232,9 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
     next.kickoff_match_order = saved.kickoff_match_order;
     next.kickoff_match_index = saved.kickoff_match_index;
     next.respawn_match_order = saved.respawn_match_order;
-    if (seed == 0) seed = saved.kickoff_resets * 0x9e3779b97f4a7c15ull;
+    const bool no_seed = how.seed_mode == 2 || (how.seed_mode == 0 && seed == 0);
+    const bool next_kickoff = no_seed && how.preserve_score && (saved.kickoff_match_order & 0x8000u) != 0;
+    if (no_seed) seed = saved.kickoff_resets * 0x9e3779b97f4a7c15ull;
     next.car_visit_order_mode = saved.car_visit_order_mode;
     next.car_visit_order_packed = saved.car_visit_order_packed;
     if (saved.car_visit_order_mode == 3) {
@@ -199,21 +243,51 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
     }
     next.frame_ticks = saved.frame_ticks;
     next.frame_frac_prev = saved.frame_frac_prev;
-    int kickoff_order[5];
-    build_kickoff_order(seed, env_idx, kickoff_order);
-    {
-        uint32_t packed = 0x8000u;
-        for (int j = 0; j < 5; ++j) packed |= static_cast<uint32_t>(kickoff_order[j]) << (3 * j);
-        next.kickoff_match_order = static_cast<uint16_t>(packed);
-        next.kickoff_match_index = 1;
-        next.respawn_match_order = build_respawn_order(seed, env_idx);
+    if (how.preserve_score) {
+        next.blue_score = saved.blue_score;
+        next.orange_score = saved.orange_score;
+        next.tick = saved.tick;
+        next.last_scored_team = saved.last_scored_team;
+    }
+    int blue_count = 0, orange_count = 0;
+    for (int k = 0; k < count; ++k) {
+        if (teams[reset_visit_slot(next, k, count)] == 0)
+            ++blue_count;
+        else
+            ++orange_count;
+    }
+    int kickoff_order[5] = {0, 1, 2, 3, 4};
+    if (how.seed_mode == 3) {
+    } else if (next_kickoff) {
+        for (int j = 0; j < 5; ++j)
+            kickoff_order[j] = (saved.kickoff_match_order >> (3 * ((saved.kickoff_match_index + j) % 5))) & 7;
+    } else {
+        build_kickoff_order(seed, env_idx, kickoff_order);
+    }
+    if (how.seed_mode != 3) {
+        if (next_kickoff) {
+            next.kickoff_match_index = static_cast<uint8_t>((saved.kickoff_match_index + 1) % 5);
+        } else {
+            uint32_t packed = 0x8000u;
+            for (int j = 0; j < 5; ++j) packed |= static_cast<uint32_t>(kickoff_order[j]) << (3 * j);
+            next.kickoff_match_order = static_cast<uint16_t>(packed);
+            next.kickoff_match_index = 1;
+            next.respawn_match_order = build_respawn_order(seed, env_idx);
+        }
+    }
+    int team_order[2][5];
+    for (int j = 0; j < 5; ++j) team_order[0][j] = team_order[1][j] = kickoff_order[j];
+    if (next_kickoff && blue_count != orange_count) {
+        const int short_team = blue_count < orange_count ? 0 : 1;
+        prefer_kickoff_spot_for_short_team(team_order[short_team], short_team == 0 ? blue_count : orange_count);
     }
     env = next;
-    uint32_t order_bits = 0;
-    for (int i = 0; i < 5; ++i) order_bits |= static_cast<uint32_t>(kickoff_order[i]) << (3 * i);
+    uint32_t order_bits[2] = {0, 0};
+    for (int t = 0; t < 2; ++t)
+        for (int i = 0; i < 5; ++i) order_bits[t] |= static_cast<uint32_t>(team_order[t][i]) << (3 * i);
 
     reset_kickoff_ball(ball);
-    if (pads) {
+    if (pads && !how.keep_pads) {
         for (int p = 0; p < L.count; ++p) {
             PadState& pad = pads[p];
             pad.cooldown = 0.0f;
@@ -231,12 +305,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
         int nth = 0;
         bool found = false;
         for (int k = 0; k < count && !found; ++k) {
-            int s;
-            if (env.car_visit_order_mode == 1 || env.car_visit_order_mode == 3) {
-                s = static_cast<int>((env.car_visit_order_packed >> (4 * k)) & 0xFu);
-            } else {
-                s = env.car_visit_order_mode == 2 ? count - 1 - k : k;
-            }
+            const int s = reset_visit_slot(env, k, count);
             if (s == i) {
                 found = true;
             } else if (teams[s] == team) {
@@ -244,7 +313,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
             }
         }
         if (!found) continue;
-        const int spot = nth < 5 ? static_cast<int>((order_bits >> (3 * nth)) & 7u) : nth;
+        const int spot = nth < 5 ? static_cast<int>((order_bits[team == 0 ? 0 : 1] >> (3 * nth)) & 7u) : nth;
         SpawnPos spawn;
         if (nth >= 5) {
             // a sixth car of a team takes a respawn spot, 250 uu further back per round of four

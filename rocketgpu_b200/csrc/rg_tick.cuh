@@ -1367,8 +1367,9 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
         // cars within wheel reach of each other: vehicle updates in the game's car order, wheels seeing other cars
         for (int k = 0; k < count; ++k) {
             const int i = order[k];
+            const uint32_t excluded = A.cars[i].is_demoed ? 0u : wheel_ray_excluded_bodies(A.cars[i], A.cfgs[i], &bp, i, count);
             vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh,
-                           WheelOthers{A.cars, A.cfgs, count, i}, recs[i].pushes);
+                           WheelOthers{A.cars, A.cfgs, count, i, excluded}, recs[i].pushes);
         }
     }
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
@@ -1377,6 +1378,9 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         CarState& car = A.cars[i];
+        // a car demolished during this world step reports the rotation it had when the step began (reference
+        // StepEnvPostCar, env_step.hpp:6915-6918)
+        if (!pre[i].is_demoed && !car.just_respawned && car.is_demoed) car.rot = pre[i].rot;
         car_post_tick(car, A.controls[i], c.tick_dt);
         car_finish_tick(car);
         if (report_fields) {
@@ -1392,6 +1396,83 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     }
     apply_ball_extra_hits(b, A.cars, count, c);
     env_tail(env, b, c, A.cars, count);
+}
+
+// ---- env commands ------------------------------------------------------------------------------------------------
+// One arena's command (byte-identical to rg_env_command / the reference's EnvCommand, rocketgpu.h:683-706).
+struct EnvCommand {
+    uint8_t reset_to_kickoff, reset_scoreboard, reset_tick_count, kickoff_seed_mode, new_round_bodies, keep_boost_pads;
+    uint16_t kickoff_countdown_ticks;
+    uint64_t kickoff_seed;
+};
+static_assert(sizeof(EnvCommand) == sizeof(rg_env_command), "EnvCommand layout");
+
+RG_HD bool env_command_active(const EnvCommand& c) {
+    return (c.reset_to_kickoff | c.reset_scoreboard | c.reset_tick_count | c.new_round_bodies) != 0;
+}
+
+// The persistent contact state of one arena an env command may clear.
+struct ArenaContactState {
+    BallWorldScratch* ball_world;
+    Broadphase* bp;
+    CarWorldScratch* car_world;  // max_cars entries
+    BallCarScratch* ball_car;    // max_cars entries
+    CarCarManifold* pairs;       // pair_slots entries (may be null)
+    int pair_slots;
+};
+
+RG_HDI void clear_retained_car_contacts(const ArenaContactState& s, int max_cars) {
+    for (int k = 0; k < max_cars; ++k) {
+        s.car_world[k].count = 0;
+        s.ball_car[k].count = 0;
+    }
+    for (int k = 0; s.pairs && k < s.pair_slots; ++k) s.pairs[k].count = 0;
+}
+
+// An arena's env command between ticks (reference ApplyEnvCommandBodies + ApplyEnvCommand + ApplyEnvCommandEnvState,
+// env_step.hpp:5672-5758, as BatchSim applies them, src/rocketgpu.cpp:2136-2218 and the tick-start command of
+// StepEnvPreTickEnv, env_step.hpp:6701-6749):
+//   * the bodies: a reset with the scoreboard starts a fresh sweep; a reset without it, or new_round_bodies, takes
+//     every body out of the sweep the way the game respawns them after a goal (demolished cars first), and the
+//     ball's and the cars' retained contacts start over;
+//   * reset_to_kickoff: the arena's kickoff (the match's next kickoff when the scoreboard is kept and no seed is
+//     given), every retained contact cleared, then the scoreboard / tick counter / countdown fields of the env.
+// A command without reset_to_kickoff changes no env field (the reference applies the env fields only with a reset).
+// kickoff_countdown_ticks must be 0 (the game's countdown spawn is not built; the batch refuses others).
+RG_HDI void apply_env_command(const EnvCommand& cmd, int env_idx, EnvState& env, BallState& ball,
+                              const ArenaContactState& cs, const ArenaCars& A, CarControls* controls,
+                              const PadLayout& L, const TickConfig& tc) {
+    if (!env_command_active(cmd)) return;
+    const int count = A.count;
+    if (cmd.reset_to_kickoff && cmd.reset_scoreboard) {
+        memset(cs.bp, 0, sizeof(Broadphase));
+    } else if (cmd.reset_to_kickoff || cmd.new_round_bodies) {
+        uint8_t demoed[8];
+        for (int i = 0; i < count && i < 8; ++i) demoed[i] = A.cars[i].is_demoed;
+        bp_new_round(*cs.bp, count, demoed);
+        memset(cs.ball_world, 0, sizeof(BallWorldScratch));
+        clear_retained_car_contacts(cs, A.max_cars);
+    }
+    if (!cmd.reset_to_kickoff) return;
+    KickoffReset how;
+    how.preserve_score = cmd.reset_scoreboard == 0;
+    how.seed_mode = cmd.kickoff_seed_mode;
+    how.keep_pads = cmd.keep_boost_pads != 0;
+    reset_env_to_kickoff(env_idx, cmd.kickoff_seed, env, ball, *cs.ball_world, A.cars, A.cfgs, controls, A.pads, L,
+                         A.teams, count, A.max_cars, tc, how);
+    clear_retained_car_contacts(cs, A.max_cars);
+    for (int k = 0; k < count; ++k) A.cars[car_visit_slot(env, k, count)].driving_disabled = 0;
+    ball.constrained_2d = 0;
+    if (cmd.reset_scoreboard) {
+        env.blue_score = 0;
+        env.orange_score = 0;
+        env.last_scored_team = -1;
+    }
+    if (cmd.reset_tick_count) env.tick = 0;
+    env.goal_scored_this_tick = 0;
+    env.countdown_phase = 0;
+    env.countdown_fires = 0;
+    env.countdown_count = 0.0f;
 }
 
 }  // namespace rg

@@ -7,6 +7,7 @@
 // (how BatchSim runs it). Three-wheel (Psyclops) cars and per-wheel state-set normals are not built.
 #pragma once
 
+#include "rg_broadphase.cuh"
 #include "rg_car.cuh"
 
 namespace rg {
@@ -269,12 +270,56 @@ RG_HDI bool wheel_ray_vs_ball(V3 src_bt, V3 dir, float max_len, const BallState&
     return true;
 }
 
-// The other cars of the arena a wheel ray may land on (null `cars`: none within reach, see arena_wheel_reach_near).
+// The other cars of the arena a wheel ray may land on (null `cars`: none within reach, see arena_wheel_reach_near),
+// and the bodies (bit 0 the ball, bit i + 1 car slot i) the car's rays skip this tick (wheel_ray_excluded_bodies).
 struct WheelOthers {
     CarState* cars;
     const CarConfig* cfgs;
     int count, self;
+    uint32_t excluded;
 };
+
+// The bodies a car's suspension rays skip this tick: those whose swept AABB from the arena's last sweep misses the
+// box around all four of the car's rays (reference WheelRayExcludedBodies with WheelRaysWhole,
+// raycast_wheels_and_contact_prep.hpp:9-25, 508-606, as StepEnvVehicleUpdateCarInline calls it, env_step.hpp:6232).
+// The ball is body 0, car slot i body i + 1; bodies without a stored box (not yet swept, or left the sweep) are tested.
+RG_HDI uint32_t wheel_ray_excluded_bodies(const CarState& c, const CarConfig& cfg, const Broadphase* bp, int self,
+                                          int count) {
+    const int bodies = count + 1 < kBpBodies ? count + 1 : kBpBodies;
+    const uint32_t mask = (bp != nullptr && bodies > 0)
+                              ? (bp->body_aabb_valid & ((1u << bodies) - 1u) & ~(1u << (self + 1)))
+                              : 0u;
+    if (mask == 0u) return 0u;
+    V3 fw, rt, up;
+    car_basis(c, fw, rt, up);
+    const V3 dir = -up;
+    const float oz = cfg.hitbox_offset.z;
+    float front_bone, back_bone;
+    wheel_bone_z(cfg, front_bone, back_bone);
+    const float front_len_bt =
+        ((oz - front_bone) * kUuToBt + cfg.front_wheel_radius * kUuToBt) + ((14.5f - kWheelSuspensionSubtraction) * kUuToBt);
+    const float back_len_bt =
+        ((oz - back_bone) * kUuToBt + cfg.back_wheel_radius * kUuToBt) + ((14.5f - kWheelSuspensionSubtraction) * kUuToBt);
+    V3 mn{0.0f, 0.0f, 0.0f}, mx{0.0f, 0.0f, 0.0f};
+    for (int i = 0; i < 4; ++i) {
+        V3 offset = i < 2 ? cfg.front_wheels_offset : cfg.back_wheels_offset;
+        if (i % 2) offset.y = -offset.y;
+        offset.z = oz;
+        const V3 from = c.pos_bt + rotate_via_basis(fw, rt, up, offset * kUuToBt);
+        const V3 to = from + dir * (i < 2 ? front_len_bt : back_len_bt);
+        const V3 lo = vmin(from, to), hi = vmax(from, to);
+        mn = i == 0 ? lo : vmin(mn, lo);
+        mx = i == 0 ? hi : vmax(mx, hi);
+    }
+    uint32_t excluded = 0u;
+    for (int body = 0; body < bodies; ++body) {
+        if (!((mask >> body) & 1u)) continue;
+        const float* a = bp->body_aabb[body];
+        if (a[3] < mn.x || mx.x < a[0] || a[4] < mn.y || mx.y < a[1] || a[5] < mn.z || mx.z < a[2])
+            excluded |= 1u << body;
+    }
+    return excluded;
+}
 
 // Distance from a point to a car's hitbox (core box plus margin) by Bullet's GJK pair detector with the Voronoi
 // simplex solver; keeps the result only when it is nearer than `out_distance` (reference WheelGjkPointBoxClosest,
@@ -483,7 +528,7 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
         int best_idx = -1;
         bool best_nr = false;
         for (int i = 0; i < oth.count; ++i) {
-            if (i == oth.self) continue;
+            if (i == oth.self || ((oth.excluded >> (i + 1)) & 1u)) continue;
             const CarState& o = oth.cars[i];
             if (o.is_demoed) continue;
             {
@@ -512,7 +557,7 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
             selected_no_response = best_nr;
         }
     }
-    {
+    if (!(oth.excluded & 1u)) {
         RayHit bh;
         if (wheel_ray_vs_ball(w.ray_source_bt, w.wheel_dir_ws, real_ray_length, ball, tc.ball_radius,
                               real_ray_length_bt, bh)) {

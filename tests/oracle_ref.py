@@ -132,6 +132,11 @@ class OracleSim:
         c = np.ascontiguousarray(ctrl, np.uint8)
         _check(lib().orc_step_with_controls(self.h, _ptr(c), ticks, stride))
 
+    def step_with_commands(self, ctrl: np.ndarray, ctrl_stride: int, cmds: np.ndarray, cmd_stride: int, ticks: int):
+        c = np.ascontiguousarray(ctrl, np.uint8)
+        m = np.ascontiguousarray(cmds, np.uint8)
+        _check(lib().orc_step_with_commands(self.h, _ptr(c), ctrl_stride, _ptr(m), cmd_stride, ticks))
+
     def _down(self, fn, n, nbytes):
         out = np.zeros((n, nbytes), np.uint8)
         _check(fn(self.h, _ptr(out), n))

@@ -126,3 +126,54 @@ def chase_ball_controls(cars: np.ndarray, balls: np.ndarray, max_cars: int, rng:
     ctrl[:, 20] = rng.random(n) < p_jump
     ctrl[:, 21] = 1
     return ctrl
+
+
+# ---- episodes ---------------------------------------------------------------------------------------------------------
+ENV_COMMAND_BYTES = 16
+CAR_LATEST_TOUCH = 520  # CarState.latest_touch_tick (u64)
+ENV_TICK, ENV_BLUE, ENV_ORANGE = 0, 4, 8
+
+
+def _splitmix(x: np.ndarray) -> np.ndarray:
+    x = (x + np.uint64(0x9E3779B97F4A7C15)).astype(np.uint64)
+    x = ((x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)).astype(np.uint64)
+    x = ((x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)).astype(np.uint64)
+    return x ^ (x >> np.uint64(31))
+
+
+class EpisodeClock:
+    """Host statement of rg_batch_episode_commands for the oracle side: after each step, an env whose score is non-zero
+    (a goal this episode) or whose ball no car touched for `no_touch_ticks` ticks gets a fresh-episode reset
+    (reset_to_kickoff = reset_scoreboard = reset_tick_count = 1) for the next step's first tick. Touches are seen
+    through each car's latest_touch_tick changing between checks; `stagger_seed` starts each env's clock at a seeded
+    age in [0, no_touch_ticks)."""
+
+    def __init__(self, envs: np.ndarray, cars: np.ndarray, max_cars: int, no_touch_ticks: int, stagger_seed: int = 0):
+        n = envs.shape[0]
+        self.max_cars, self.no_touch = max_cars, no_touch_ticks
+        self.seen = cars[:, CAR_LATEST_TOUCH:CAR_LATEST_TOUCH + 8].copy().view(np.uint64).reshape(n, max_cars)
+        tick = envs[:, ENV_TICK:ENV_TICK + 4].copy().view(np.uint32).ravel().astype(np.int64)
+        age = np.zeros(n, np.int64)
+        if stagger_seed:
+            with np.errstate(over="ignore"):
+                h = _splitmix(np.uint64(stagger_seed) ^ np.arange(n, dtype=np.uint64))
+            age = (h % np.uint64(no_touch_ticks)).astype(np.int64)
+        self.touch = tick - age
+
+    def commands(self, envs: np.ndarray, cars: np.ndarray, counts: np.ndarray) -> np.ndarray:
+        n = envs.shape[0]
+        latest = cars[:, CAR_LATEST_TOUCH:CAR_LATEST_TOUCH + 8].copy().view(np.uint64).reshape(n, self.max_cars)
+        active = np.arange(self.max_cars)[None, :] < np.asarray(counts)[:, None]
+        changed = active & (latest != self.seen)
+        self.seen = np.where(changed, latest, self.seen)
+        valid = changed & (latest != np.uint64(0xFFFFFFFFFFFFFFFF))
+        cand = np.where(valid, latest.astype(np.int64), np.iinfo(np.int64).min)
+        self.touch = np.maximum(self.touch, cand.max(axis=1))
+        tick = envs[:, ENV_TICK:ENV_TICK + 4].copy().view(np.uint32).ravel().astype(np.int64)
+        score = envs[:, ENV_BLUE:ENV_BLUE + 4].copy().view(np.uint32).ravel() | \
+            envs[:, ENV_ORANGE:ENV_ORANGE + 4].copy().view(np.uint32).ravel()
+        reset = (score != 0) | (tick - self.touch >= self.no_touch)
+        self.touch = np.where(reset, 0, self.touch)
+        out = np.zeros((n, ENV_COMMAND_BYTES), np.uint8)
+        out[reset, 0:3] = 1
+        return out

@@ -68,9 +68,34 @@ def test_invalid_config_is_rejected_before_any_device_call(arena_mesh):
         BatchSim(SimConfig(env_count=0), v, i)
     with pytest.raises(ValueError):
         BatchSim(SimConfig(env_count=4, max_cars_per_env=9), v, i)
+    # 7- and 8-car arenas would overflow the car-car pair rows; kickoff settling is not built
+    with pytest.raises(ValueError):
+        BatchSim(SimConfig(env_count=4, max_cars_per_env=7), v, i)
+    with pytest.raises(ValueError, match="kickoff_settled"):
+        BatchSim(SimConfig(env_count=4, kickoff_settled=1), v, i)
+    assert SimConfig().c.kickoff_settled == 0
     with pytest.raises(ValueError):
         BatchSim(SimConfig(env_count=4), v, i[:-1])
     bad = v.copy()
     bad[0, 0] = 12000.0
     with pytest.raises(ValueError):
         BatchSim(SimConfig(env_count=4), bad, i)
+
+
+def test_parity_compare_allows_only_nan_payloads():
+    from tests import parity
+    a = np.zeros(16, np.uint8)
+    a[0:4] = np.frombuffer(np.float32(1.5).tobytes(), np.uint8)
+    a[4:8] = np.frombuffer(np.uint32(0xffc00000).tobytes(), np.uint8)  # x86 NaN
+    b = a.copy()
+    b[4:8] = np.frombuffer(np.uint32(0x7fffffff).tobytes(), np.uint8)  # GPU NaN
+    assert parity.equal(a, b)
+    c = b.copy()
+    c[0:4] = np.frombuffer(np.float32(1.5000001).tobytes(), np.uint8)  # one ulp
+    assert parity.mismatched_bytes(a, c).tolist() == [0]
+    d = a.copy()
+    d[4:8] = np.frombuffer(np.float32(2.0).tobytes(), np.uint8)  # NaN on one side only
+    assert not parity.equal(a, d)
+    e = a.copy()
+    e[15] = 1
+    assert parity.mismatched_bytes(a, e).tolist() == [15]
