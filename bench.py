@@ -2,23 +2,39 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload mixed|balls]
 
-Workload `mixed` (default): 16,384 arenas per GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3 (seeded), default car body, in
-the procedural ~11k-triangle arena, started with reset_to_kickoff. Controls come from the seeded generator (throttle,
-steer, pitch, yaw, roll U[-1, 1]; jump / boost / handbrake Bernoulli 0.1 / 0.3 / 0.1; each sample held for U{1..30}
-ticks). A step is one BatchSim::step_with_device_controls of 8 ticks (one kernel launch) over a [8, car_capacity]
-control block resident in HBM. Workload `balls`: 16,384 ball-only arenas, balls at seeded positions with seeded
-velocities up to 6000 uu/s, 8 ticks per step.
+Workload `mixed` (default): 16,384 arenas per GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3 (seeded), car bodies drawn
+uniformly from the six hitbox presets (Octane, Dominus, Plank, Breakout, Hybrid, Merc), in the procedural ~11k-triangle
+arena. Controls come from the seeded generator (throttle, steer, pitch, yaw, roll U[-1, 1]; jump / boost / handbrake
+Bernoulli 0.1 / 0.3 / 0.1; each sample held for U{1..30} ticks). An arena resets to kickoff when its ball is scored or
+when no car has touched the ball for 300 ticks; the no-touch clocks start at seeded ages, so resets are spread over the
+ticks. A step is 8 ticks: one BatchSim::step_with_device_commands over a [8, car_capacity] control block resident in
+HBM, whose first tick applies the resets rg_batch_episode_commands chose after the previous step (4 kernels per tick
+plus the episode kernel, 33 launches per step).
+
+Steady state: every arena starts from kickoff, so SETTLE_STEPS untimed steps (320 ticks) run first, then W warm-up
+steps; the K timed steps follow. Every pass (the device-timed pass, the end-to-end pass and the CPU baseline / the
+reference arm) runs the same settle and warm-up and then times the same K steps, so all numbers cover the same ticks.
+
+Workload `balls`: 16,384 ball-only arenas, balls at seeded positions with seeded velocities up to 6000 uu/s, 8 ticks
+per step (one launch).
 
 Arenas are independent, so N GPUs run N shards of 16,384 arenas each ("scaling": "weak") with no data-path collective;
 the only cross-rank traffic is the timing max-reduction.
 
-Timing: W untimed warm-up steps; then K steps, each timed with CUDA events on the launching stream after a 256 MiB L2
-flush (outside the events), barrier + synchronize around the timed region, max over ranks. `e2e` times the same steps
-through the public API from host code: each step copies its control block from pinned host memory to the device and
-reads every car and ball state back into pinned memory (the observation), both inside the timed region.
+Timing: K steps, each timed with CUDA events on the launching stream after a 256 MiB L2 flush (outside the events),
+barrier + synchronize around the timed region, max over ranks; p50 / p99 of the per-step times. `e2e` times the same
+K steps through the public API on a second batch brought to the same state: each step copies its control block from
+pinned host memory to the device, steps, and reads every car and ball state back into pinned memory, all inside the
+timed region (host wall clock).
 
-`--impl reference` times the reference's own CPU implementation (oracle/_ref, built from the reference's sources) on
-the same workload with all host threads, on a bounded sample of steps.
+Parity: rank 0 at N=1 steps the oracle (the reference's own CPU BatchSim, oracle/_ref) through the same settle,
+warm-up and K steps with the same controls and the same reset decisions (made on the host from the oracle's state),
+and compares every arena's cars and ball after each of the K steps of the end-to-end pass, and every arena's cars,
+ball, env and pads at the end of the device-timed pass, bitwise (NaN payloads aside). The oracle's K step calls,
+timed, are the CPU baseline.
+
+`--impl reference` runs that CPU leg alone and reports it (the reference's own CPU implementation with all host
+threads, on the same workload, settle, warm-up and timed steps).
 """
 from __future__ import annotations
 
@@ -38,18 +54,27 @@ sys.path.insert(0, ROOT)
 
 ENVS = 16384
 TICKS_PER_STEP = 8
+SETTLE_STEPS = 40
+NO_TOUCH_TICKS = 300
 MAX_CARS = 6
 METRIC = "arena-ticks/s"
-CAR_BYTES, BALL_BYTES, ENV_BYTES, WHEEL_BYTES, CAR_MANIFOLD_BYTES, CTRL_BYTES, PAD_BYTES = 880, 288, 44, 292, 208, 24, 16
+CAR_BYTES, BALL_BYTES, ENV_BYTES, PAD_BYTES, CTRL_BYTES, CMD_BYTES = 880, 288, 44, 16, 24, 16
 WORKLOADS = {
-    "mixed": "16384 arenas/GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3 from kickoff, seeded held controls, procedural "
-             "11k-tri arena, 8 ticks per launch",
+    "mixed": "16384 arenas/GPU mixed 55% 1v1 / 27% 2v2 / 18% 3v3, six hitbox presets, goal or 300-tick no-touch "
+             "resets (staggered clocks), seeded held controls, procedural 11k-tri arena, 8 ticks per step, "
+             "320-tick settle before warm-up",
     "balls": "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step",
 }
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per step, from the ncu captures summarised under profiles/:
-# balls, one tick_kernel launch of 8 ticks at 16,384 arenas; mixed, arena_finish + car_vehicle per tick at 4,096
-# arenas times 8 ticks, scaled by 4 to 16,384 arenas (profiles/tick_kernels_mixed_car_arenas.md)
-TRAFFIC_PER_LAUNCH = {"balls": 16.01e6, "mixed": 1.72e9}
+# Algorithmic bytes of one arena_finish_kernel launch (one tick), read + write of the state it owns:
+# per arena ball 288, ball contact state 288, env 44, broadphase history 1,344, 34 pads x 16, tick snapshot 24;
+# per active car its state 880, wheel record 292, car/mesh manifold 208, car/ball manifold 208, tick record 148, and
+# its control row 24 read once; per car pair (n(n-1)/2 of the arena's n cars) its manifold 260.
+FINISH_BYTES_PER_ARENA = 2 * (288 + 288 + 44 + 1344 + 34 * 16) + 24
+FINISH_BYTES_PER_CAR = 2 * (880 + 292 + 208 + 208 + 148) + 24
+FINISH_BYTES_PER_PAIR = 2 * 260
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one arena_finish_kernel launch at 16,384 arenas, from
+# the ncu capture summarised in profiles/ (a 4,096-arena capture scaled by 4); None until captured.
+FINISH_TRAFFIC = None
 
 
 def peaks():
@@ -80,6 +105,7 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -138,32 +164,141 @@ def barrier(world):
         dist.barrier()
 
 
-# ---- the mixed workload's inputs (shared by both arms) -----------------------------------------------------------
-def mixed_layout(seed: int):
-    """Cars per arena (2/4/6 with p = .55/.27/.18) and teams (the first half of an arena's cars blue, the rest
-    orange)."""
-    rng = np.random.default_rng(seed)
-    counts = rng.choice(np.array([2, 4, 6], np.int32), size=ENVS, p=[0.55, 0.27, 0.18]).astype(np.int32)
-    teams = np.zeros(ENVS * MAX_CARS, np.uint8)
-    for n in (2, 4, 6):
-        idx = np.nonzero(counts == n)[0]
-        for s in range(n // 2, n):
-            teams[idx * MAX_CARS + s] = 1
-    return counts, teams
+# ---- the mixed workload's inputs (shared by every pass) ----------------------------------------------------------
+class MixedWorkload:
+    """Cars per arena (2/4/6 with p = .55/.27/.18), teams (the first half of an arena's cars blue), car bodies (uniform
+    over the six presets), and the seeded control stream, for shard `rank`."""
+
+    def __init__(self, rank: int):
+        rng = np.random.default_rng(7 + rank)
+        self.counts = rng.choice(np.array([2, 4, 6], np.int32), size=ENVS, p=[0.55, 0.27, 0.18]).astype(np.int32)
+        self.teams = np.zeros(ENVS * MAX_CARS, np.uint8)
+        for n in (2, 4, 6):
+            idx = np.nonzero(self.counts == n)[0]
+            for s in range(n // 2, n):
+                self.teams[idx * MAX_CARS + s] = 1
+        self.bodies = rng.integers(0, 6, ENVS * MAX_CARS)
+        self.reset_seed = 1000 + rank
+        self.control_seed = 2000 + rank
+        self.stagger_seed = 3000 + rank
+
+    def car_configs(self, presets: list[np.ndarray]) -> np.ndarray:
+        return np.stack(presets)[self.bodies]
+
+    def controls(self):
+        """Generator of [TICKS_PER_STEP * capacity, 24] control blocks, one per step from the first settle step."""
+        from tests import scenarios
+        stream = scenarios.ControlStream(ENVS * MAX_CARS, seed=self.control_seed, p_jump=0.1, hold_max=30)
+        while True:
+            yield np.stack([stream.next() for _ in range(TICKS_PER_STEP)]).reshape(-1, CTRL_BYTES)
 
 
-def control_blocks(n_steps: int, seed: int) -> np.ndarray:
-    """[n_steps, TICKS_PER_STEP, capacity, 24] control rows from the seeded generator (held U{1..30} ticks)."""
-    from tests import scenarios
-    cap = ENVS * MAX_CARS
-    stream = scenarios.ControlStream(cap, seed=seed, p_jump=0.1, hold_max=30)
-    out = np.empty((n_steps, TICKS_PER_STEP, cap, CTRL_BYTES), np.uint8)
-    for s in range(n_steps):
-        for t in range(TICKS_PER_STEP):
-            out[s, t] = stream.next()
-    return out
+def _presets():
+    """The six hitbox presets as the oracle exports them (byte-identical CarConfig rows)."""
+    from tests import oracle_ref
+    return [oracle_ref.car_preset(k) for k in range(6)]
 
 
+def arena_hashes(rows: np.ndarray, per_arena: int) -> np.ndarray:
+    """One 64-bit polynomial hash per arena of its rows (NaN words canonicalised), for per-step parity checks."""
+    flat = np.ascontiguousarray(rows).reshape(ENVS, -1)
+    pad = (-flat.shape[1]) % 8
+    if pad:
+        flat = np.concatenate([flat, np.zeros((ENVS, pad), np.uint8)], axis=1)
+    w32 = flat.view(np.uint32).copy()
+    w32[np.isnan(w32.view(np.float32))] = 0x7FC00000
+    w = w32.view(np.uint64)
+    k = (np.arange(w.shape[1], dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)) | np.uint64(1)
+    with np.errstate(over="ignore"):
+        return (w * k).sum(axis=1, dtype=np.uint64) ^ (w ^ k).sum(axis=1, dtype=np.uint64)
+
+
+def _active_car_rows(cars: np.ndarray, counts: np.ndarray) -> np.ndarray:
+    """Car rows with the inactive slots zeroed (they are not part of the comparison)."""
+    c = cars.reshape(ENVS, MAX_CARS, CAR_BYTES).copy()
+    c[np.arange(MAX_CARS)[None, :] >= counts[:, None]] = 0
+    return c
+
+
+# ---- the CPU leg: the reference's own CPU BatchSim --------------------------------------------------------------
+def oracle_lib_path():
+    """The timed CPU build (-march=x86-64-v3) when it loads on this host, else the portable one."""
+    from tests import oracle_ref
+    native = os.path.join(ROOT, "oracle", "_ref", "librg_oracle_native.so")
+    if os.path.exists(native):
+        try:
+            ctypes.CDLL(native)
+            return native, "x86-64-v3"
+        except OSError:
+            pass
+    return oracle_ref.LIB_PATH, "x86-64"
+
+
+def cpu_leg(workload: str, warmup: int, steps: int, parity: bool):
+    """Runs the reference's CPU BatchSim through the settle, warm-up and `steps` timed steps of the workload with all
+    host threads. Returns the timing record and, with `parity`, the per-step arena hashes and the final state."""
+    from rocketgpu_b200 import arena
+    from tests import oracle_ref, scenarios
+    if not oracle_ref.available():
+        return {"value": None, "unit": "arena-ticks/s", "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref not built"}, None
+    cores = os.cpu_count() or 1
+    os.environ["ROCKETGPU_CPU_THREADS"] = str(cores)
+    path, arch = oracle_lib_path()
+    if oracle_ref.LIB_PATH != path:
+        oracle_ref.LIB_PATH = path
+        oracle_ref._lib = None
+    v, i = arena.generate()
+    record = {"hashes": [], "final": None}
+    step_s = []
+    if workload == "mixed":
+        w = MixedWorkload(0)
+        sim = oracle_ref.OracleSim(ENVS, MAX_CARS, v, i, kickoff_settled=False)
+        sim.set_env_car_count(w.counts)
+        sim.set_teams(w.teams)
+        sim.set_car_configs(w.car_configs(_presets()))
+        sim.reset_to_kickoff(w.reset_seed)
+        clock = scenarios.EpisodeClock(sim.envs(), sim.cars(), MAX_CARS, NO_TOUCH_TICKS, w.stagger_seed)
+        cmds = np.zeros((TICKS_PER_STEP * ENVS, CMD_BYTES), np.uint8)
+        gen = w.controls()
+        total = SETTLE_STEPS + warmup + steps
+        for k in range(total):
+            block = next(gen)
+            t0 = time.perf_counter()
+            sim.step_with_commands(block, ENVS * MAX_CARS, cmds, ENVS, TICKS_PER_STEP)
+            dt = time.perf_counter() - t0
+            cars, envs = sim.cars(), sim.envs()
+            timed = k >= SETTLE_STEPS + warmup
+            if timed:
+                step_s.append(dt)
+                if parity:
+                    record["hashes"].append((arena_hashes(_active_car_rows(cars, w.counts), MAX_CARS * CAR_BYTES),
+                                             arena_hashes(sim.balls(), BALL_BYTES)))
+            cmds[:ENVS] = clock.commands(envs, cars, w.counts)
+        if parity:
+            record["final"] = (_active_car_rows(sim.cars(), w.counts), sim.balls(), sim.envs(), sim.pads())
+    else:
+        sim = oracle_ref.OracleSim(ENVS, 2, v, i, kickoff_settled=False)
+        sim.set_env_car_count([0] * ENVS)
+        _, default_ball, _, _, _ = oracle_ref.default_states()
+        sim.upload_balls(scenarios.ball_states(default_ball, ENVS, seed=1000))
+        for k in range(warmup + steps):
+            t0 = time.perf_counter()
+            sim.step(TICKS_PER_STEP)
+            if k >= warmup:
+                step_s.append(time.perf_counter() - t0)
+        if parity:
+            record["final"] = (None, sim.balls(), sim.envs(), None)
+    sim.close()
+    value = ENVS * TICKS_PER_STEP * len(step_s) / sum(step_s)
+    timing = {"value": value, "unit": "arena-ticks/s", "cores": cores, "kind": "reference",
+              "sample": f"the timed {len(step_s)} steps x {TICKS_PER_STEP} ticks x {ENVS} arenas ({workload}) after "
+                        f"the same settle and warm-up, step calls only, ROCKETGPU_CPU_THREADS={cores}, oracle built "
+                        f"for {arch}"}
+    return timing, record
+
+
+# ---- our arm ------------------------------------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
     import torch
 
@@ -177,171 +312,211 @@ def run_ours(args, world, rank, local):
     s_handle = ctypes.c_void_p(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     mixed = args.workload == "mixed"
-    n_steps = args.warmup + args.steps
-    if mixed:
-        sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=MAX_CARS, kickoff_settled=0), v, i, device=local)
-        counts, teams = mixed_layout(seed=7 + rank)
-        sim.set_env_car_count(counts)
-        sim.set_teams(teams)
-        sim.reset_to_kickoff(1000 + rank)
-        cap = sim.car_capacity()
-        blocks_host = control_blocks(n_steps, seed=2000 + rank)
-        blocks_dev = torch.from_numpy(blocks_host.reshape(n_steps, -1)).to("cuda")
-        cars_total = int(counts.sum())
-    else:
+
+    def check(rc):
+        if rc != 0:
+            raise RuntimeError(lib.rg_last_error().decode())
+
+    w = MixedWorkload(rank) if mixed else None
+    presets = _presets() if mixed else None
+
+    def make_sim():
+        if mixed:
+            sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=MAX_CARS), v, i, device=local)
+            sim.set_env_car_count(w.counts)
+            sim.set_teams(w.teams)
+            sim.set_car_configs(w.car_configs(presets))
+            sim.reset_to_kickoff(w.reset_seed)
+            cmds = torch.zeros((TICKS_PER_STEP, ENVS, CMD_BYTES), dtype=torch.uint8, device="cuda")
+            check(lib.rg_batch_episode_commands(sim._h, NO_TOUCH_TICKS, w.stagger_seed, 1,
+                                                ctypes.c_void_p(cmds.data_ptr()), s_handle))
+            return sim, cmds
         from tests import scenarios
         sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=2), v, i, device=local)
         sim.set_env_car_count(np.zeros(ENVS, np.int32))
         default_ball = np.zeros(BALL_BYTES, np.uint8)
         lib.rg_default_ball_state(default_ball.ctypes.data)
         sim.upload_ball_states(scenarios.ball_states(default_ball, ENVS, seed=1000 + rank))
-        cap, cars_total = 0, 0
+        return sim, None
 
-    def step(k, ctrl_ptr=None):
+    cap = ENVS * MAX_CARS
+
+    def step(sim, cmds, ctrl_ptr):
         if mixed:
-            ptr = ctrl_ptr if ctrl_ptr is not None else blocks_dev[k].data_ptr()
-            rc = lib.rg_batch_step_with_device_controls(sim._h, ctypes.c_void_p(ptr), TICKS_PER_STEP, cap, s_handle)
+            check(lib.rg_batch_step_with_device_commands(sim._h, ctypes.c_void_p(ctrl_ptr), cap,
+                                                         ctypes.c_void_p(cmds.data_ptr()), ENVS, TICKS_PER_STEP,
+                                                         s_handle))
+            check(lib.rg_batch_episode_commands(sim._h, NO_TOUCH_TICKS, 0, 0, ctypes.c_void_p(cmds.data_ptr()),
+                                                s_handle))
         else:
-            rc = lib.rg_batch_step(sim._h, TICKS_PER_STEP, s_handle)
-        if rc != 0:
-            raise RuntimeError(lib.rg_last_error().decode())
+            check(lib.rg_batch_step(sim._h, TICKS_PER_STEP, s_handle))
 
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-    # device-timed region
+    # the timed steps' control blocks, resident in HBM (device pass) and in pinned host memory (end-to-end pass)
+    settle = SETTLE_STEPS if mixed else 0
+    pre_steps = settle + args.warmup
+    gen = w.controls() if mixed else None
+    ctrl_dev = torch.empty(cap * TICKS_PER_STEP * CTRL_BYTES, dtype=torch.uint8, device="cuda") if mixed else None
+    pre_blocks = []
+    timed_pin = None
+    if mixed:
+        for k in range(pre_steps):
+            pre_blocks.append(next(gen))
+        timed_pin = torch.empty((args.steps, cap * TICKS_PER_STEP * CTRL_BYTES), dtype=torch.uint8, pin_memory=True)
+        for k in range(args.steps):
+            timed_pin[k].copy_(torch.from_numpy(next(gen).reshape(-1)))
+        timed_dev = timed_pin.to("cuda")
+
+    def bring_up():
+        sim, cmds = make_sim()
+        for k in range(pre_steps):
+            if mixed:
+                ctrl_dev.copy_(torch.from_numpy(pre_blocks[k].reshape(-1)))
+                step(sim, cmds, ctrl_dev.data_ptr())
+            else:
+                step(sim, None, None)
+        torch.cuda.synchronize()
+        return sim, cmds
+
+    # device-timed pass
+    sim_a, cmds_a = bring_up()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if mixed:
+        check(lib.rg_batch_phase_timing(sim_a._h, 1))
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
-            step(args.warmup + k)
+            step(sim_a, cmds_a, timed_dev[k].data_ptr() if mixed else None)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
     barrier(world)
-    launch_ms = [a.elapsed_time(b) for a, b in ev]
-    dev_s = max_over_ranks(sum(launch_ms) / 1e3, world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    phase_ms = (ctypes.c_float * 4)()
+    phase_ticks = ctypes.c_int64(0)
+    if mixed:
+        check(lib.rg_batch_phase_times(sim_a._h, phase_ms, ctypes.byref(phase_ticks)))
+        check(lib.rg_batch_phase_timing(sim_a._h, 0))
+    dev_s = max_over_ranks(sum(step_ms) / 1e3, world)
     arena_ticks = ENVS * TICKS_PER_STEP * args.steps * world
     value = arena_ticks / dev_s
-
-    # end to end through the public API: per step, the H2D copy of the step's control block from pinned memory, the
-    # step, and the D2H read of every car and ball state into pinned memory; host wall time
-    ball_pin = torch.empty((ENVS, BALL_BYTES), dtype=torch.uint8, pin_memory=True)
-    h2d = 0
+    final_a = None
     if mixed:
-        car_pin = torch.empty((cap, CAR_BYTES), dtype=torch.uint8, pin_memory=True)
-        ctrl_pin = torch.from_numpy(blocks_host[args.warmup:].reshape(args.steps, -1)).pin_memory()
-        ctrl_dev = torch.empty(ctrl_pin.shape[1], dtype=torch.uint8, device="cuda")
-        h2d = ctrl_pin.shape[1]
-        # the e2e pass replays the same control blocks from the state the timed pass left: same work per step
+        final_a = (_active_car_rows(sim_a.download_car_states(), w.counts), sim_a.download_ball_states(),
+                   sim_a.download_env_states(), sim_a.download_boost_pad_states())
+    else:
+        final_a = (None, sim_a.download_ball_states(), sim_a.download_env_states(), None)
+    sim_a.close()
+
+    # end-to-end pass through the public API, on a second batch brought to the same state
+    sim_b, cmds_b = bring_up()
+    ball_pin = torch.empty((ENVS, BALL_BYTES), dtype=torch.uint8, pin_memory=True)
+    car_pin = torch.empty((max(cap, 1), CAR_BYTES), dtype=torch.uint8, pin_memory=True)
+    e2e_hashes = []
+    e2e_ms = []
     barrier(world)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     for k in range(args.steps):
+        t0 = time.perf_counter()
         if mixed:
-            ctrl_dev.copy_(ctrl_pin[k], non_blocking=True)
-            step(None, ctrl_dev.data_ptr())
-            rc = lib.rg_batch_download_car_states(sim._h, ctypes.c_void_p(car_pin.data_ptr()), cap, s_handle)
-            if rc != 0:
-                raise RuntimeError(lib.rg_last_error().decode())
+            ctrl_dev.copy_(timed_pin[k], non_blocking=True)
+            step(sim_b, cmds_b, ctrl_dev.data_ptr())
+            check(lib.rg_batch_download_car_states(sim_b._h, ctypes.c_void_p(car_pin.data_ptr()), cap, s_handle))
         else:
-            step(k)
-        rc = lib.rg_batch_download_ball_states(sim._h, ctypes.c_void_p(ball_pin.data_ptr()), ENVS, s_handle)
-        if rc != 0:
-            raise RuntimeError(lib.rg_last_error().decode())
+            step(sim_b, None, None)
+        check(lib.rg_batch_download_ball_states(sim_b._h, ctypes.c_void_p(ball_pin.data_ptr()), ENVS, s_handle))
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        if mixed and rank == 0 and world == 1 and not args.no_cpu_baseline:
+            # outside the timed region: this step's observation, hashed for the parity check
+            e2e_hashes.append((arena_hashes(_active_car_rows(car_pin.numpy(), w.counts), MAX_CARS * CAR_BYTES),
+                               arena_hashes(ball_pin.numpy(), BALL_BYTES)))
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_s = max_over_ranks(sum(e2e_ms) / 1e3, world)
     e2e = arena_ticks / e2e_s
-    d2h = ENVS * BALL_BYTES + cap * CAR_BYTES
+    h2d = cap * TICKS_PER_STEP * CTRL_BYTES if mixed else 0
+    d2h = ENVS * BALL_BYTES + (cap * CAR_BYTES if mixed else 0)
+    sim_b.close()
 
     hbm, peak_kind = peaks()
-    per_launch_ms = float(np.mean(launch_ms))
-    if mixed:
-        # algorithmic state bytes of one launch: each arena's ball, ball contact state, env, broadphase history and
-        # pads read and written once; each active car's state, wheel record and car-mesh manifold read and written
-        # once per tick, its controls read once per tick
-        per_arena = 2 * (BALL_BYTES + 288 + ENV_BYTES + 1104 + 34 * PAD_BYTES)
-        per_car_tick = 2 * (CAR_BYTES + WHEEL_BYTES + CAR_MANIFOLD_BYTES) + CTRL_BYTES
-        bytes_per_launch = ENVS * per_arena + cars_total * per_car_tick * TICKS_PER_STEP
-    else:
-        bytes_per_launch = 2 * (BALL_BYTES + 288 + ENV_BYTES) * ENVS
-    achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded kickoff arenas and controls)" if mixed else "synthetic (seeded ball states)",
+        "data": "synthetic (seeded arenas, bodies, controls and episode resets)" if mixed
+        else "synthetic (seeded ball states)",
         "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
-                   "cars_per_gpu": cars_total, "l2": "256 MiB flush before every timed step",
+                   "settle_steps": settle, "l2": "256 MiB flush before every timed step",
                    "parallelism": f"arena shards x{world}"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_kind, "traffic": TRAFFIC_PER_LAUNCH[args.workload],
-                     "note": "per step (mixed: 8 ticks x 4 launches): algorithmic state bytes / step time; the tick is "
-                             "latency bound (one thread per arena, data-dependent branches, dependent loads), not HBM "
-                             "bound"},
+        "latency_ms_per_step": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                                "max": float(np.max(step_ms)), "e2e_p50": float(np.percentile(e2e_ms, 50)),
+                                "e2e_p99": float(np.percentile(e2e_ms, 99))},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        # mixed: four kernels per tick (arena begin, per-car tick start, per-car vehicle update, arena finish);
-        # balls: one per step
-        "gpu_launches": args.steps * TICKS_PER_STEP * 4 if mixed else args.steps,
+        "gpu_launches": args.steps * (TICKS_PER_STEP * 4 + 1) if mixed else args.steps,
         "clocks": clocks.summary(),
     }
+    if mixed:
+        cars_total = int(w.counts.sum())
+        pairs_total = int((w.counts * (w.counts - 1) // 2).sum())
+        ticks = max(1, phase_ticks.value)
+        finish_ms = phase_ms[3] / ticks
+        finish_bytes = (ENVS * FINISH_BYTES_PER_ARENA + cars_total * FINISH_BYTES_PER_CAR +
+                        pairs_total * FINISH_BYTES_PER_PAIR)
+        achieved = finish_bytes / (finish_ms / 1e3) / 1e9
+        line["config"]["cars_per_gpu"] = cars_total
+        line["roofline"] = {
+            "bound": "hbm", "kernel": "arena_finish_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": peak_kind,
+            "traffic": FINISH_TRAFFIC,
+            "algorithmic_bytes_per_launch": finish_bytes, "avg_launch_ms": finish_ms,
+            "note": "the tick is bound by latency and FP32 issue of serial per-arena work, not by HBM; frac is the "
+                    "HBM fraction of the dominant kernel's algorithmic state bytes"}
+        line["kernel_ms_per_step"] = {name: phase_ms[k] / ticks * TICKS_PER_STEP for k, name in
+                                      enumerate(("arena_begin", "car_pre", "car_vehicle", "arena_finish"))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.workload, sample_steps=args.cpu_steps)
+        timing, record = cpu_leg(args.workload, args.warmup, args.steps, parity=True)
+        line["cpu_baseline"] = timing
+        if record is not None:
+            line["parity"] = parity_summary(record, e2e_hashes, final_a, mixed)
     return line
 
 
-def cpu_baseline(workload: str, sample_steps: int = 60):
-    """The reference's own CPU BatchSim (oracle/_ref) on the same workload, all host threads, a bounded sample."""
-    from rocketgpu_b200 import arena
-    from tests import oracle_ref, scenarios
-    if not oracle_ref.available():
-        return {"value": None, "unit": "arena-ticks/s", "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref not built"}
-    cores = os.cpu_count() or 1
-    os.environ["ROCKETGPU_CPU_THREADS"] = str(cores)
-    v, i = arena.generate()
-    if workload == "mixed":
-        sim = oracle_ref.OracleSim(ENVS, MAX_CARS, v, i, kickoff_settled=False)
-        counts, teams = mixed_layout(seed=7)
-        sim.set_env_car_count(counts)
-        sim.set_teams(teams)
-        sim.reset_to_kickoff(1000)
-        cap = ENVS * MAX_CARS
-        stream = scenarios.ControlStream(cap, seed=2000, p_jump=0.1, hold_max=30)
-
-        def one(k):
-            block = np.stack([stream.next() for _ in range(TICKS_PER_STEP)])
-            sim.step_with_controls(block.reshape(-1, CTRL_BYTES), TICKS_PER_STEP, cap)
-    else:
-        sim = oracle_ref.OracleSim(ENVS, 2, v, i, kickoff_settled=False)
-        sim.set_env_car_count([0] * ENVS)
-        _, default_ball, _, _, _ = oracle_ref.default_states()
-        sim.upload_balls(scenarios.ball_states(default_ball, ENVS, seed=1000))
-
-        def one(k):
-            sim.step(TICKS_PER_STEP)
-    one(0)
-    t0 = time.perf_counter()
-    for k in range(sample_steps):
-        one(k + 1)
-    dt = time.perf_counter() - t0
-    return {"value": ENVS * TICKS_PER_STEP * sample_steps / dt, "unit": "arena-ticks/s", "cores": cores,
-            "kind": "reference",
-            "sample": f"{sample_steps} steps x {TICKS_PER_STEP} ticks x {ENVS} arenas ({workload}), "
-                      f"ROCKETGPU_CPU_THREADS={cores}"}
+def parity_summary(record, e2e_hashes, final_a, mixed):
+    from tests import parity
+    bad_steps = np.zeros(ENVS, bool)
+    for (oc, ob), (gc, gb) in zip(record["hashes"], e2e_hashes):
+        bad_steps |= (oc != gc) | (ob != gb)
+    oc, ob, oe, op = record["final"]
+    gc, gb, ge, gp = final_a
+    bad_final = np.zeros(ENVS, bool)
+    for o, g in ((oc, gc), (ob, gb), (oe, ge), (op, gp)):
+        if o is None:
+            continue
+        o = o.reshape(ENVS, -1)
+        g = g.reshape(ENVS, -1)
+        diff = np.nonzero((o != g).any(axis=1))[0]
+        for e in diff:
+            if not parity.equal(o[e], g[e]):
+                bad_final[e] = True
+    return {"arenas": ENVS, "ticks_compared": len(e2e_hashes) * TICKS_PER_STEP,
+            "compared": ("every arena's active cars and ball after each timed step of the end-to-end pass, and every "
+                         "arena's cars, ball, env and pads after the device-timed pass, bitwise (NaN payloads aside)")
+            if mixed else "every arena's ball and env after the device-timed pass, bitwise",
+            "mismatched_arenas": int((bad_steps | bad_final).sum())}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return None
-    cb = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, args.cpu_steps)))
+    cb, _ = cpu_leg(args.workload, args.warmup, args.steps, parity=False)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "arena-ticks/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded kickoff arenas and controls)",
-        "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP},
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded arenas, bodies, controls and episode resets)" if args.workload == "mixed"
+        else "synthetic (seeded ball states)",
+        "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
+                   "settle_steps": SETTLE_STEPS if args.workload == "mixed" else 0},
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -351,11 +526,10 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
-    ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--arenas", type=int, default=ENVS, help="arenas per GPU (smaller cases for profiling)")
     args = ap.parse_args()

@@ -292,6 +292,14 @@ RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls
 RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64_t stagger_seed, int32_t init,
                                      rg_env_command* device_commands, void* stream);
 
+/* Per-kernel device time of the stepping path, for profiling (no counterpart in the reference). While enabled, every
+ * tick of a car step records CUDA events on the step's stream around its four kernels (arena begin, car tick start,
+ * car vehicle update, arena finish). rg_batch_phase_times waits for the last event, returns the device milliseconds
+ * of each kernel summed over the ticks since enabling or the previous call (out_ms[4]) and the tick count, and starts
+ * a new sum. Enabling or disabling also starts a new sum. */
+RG_API int rg_batch_phase_timing(rg_batch* b, int32_t enable);
+RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks);
+
 /* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch, and a device env
  * command that was refused (invalid_argument). */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);

@@ -23,7 +23,8 @@ EXPORTS = [
     "rg_batch_pad_capacity", "rg_batch_upload_pad_states", "rg_batch_download_pad_states", "rg_batch_set_car_configs",
     "rg_batch_upload_controls", "rg_batch_step_with_device_controls", "rg_batch_set_teams",
     "rg_batch_reset_to_kickoff", "rg_batch_apply_env_commands", "rg_batch_apply_env_commands_device",
-    "rg_batch_step_with_device_commands", "rg_batch_episode_commands",
+    "rg_batch_step_with_device_commands", "rg_batch_episode_commands", "rg_batch_phase_timing",
+    "rg_batch_phase_times",
 ]
 
 
@@ -103,5 +104,7 @@ def lib():
         L.rg_batch_apply_env_commands_device.argtypes = [vp, vp, sz, vp]
         L.rg_batch_step_with_device_commands.argtypes = [vp, vp, i32, vp, i32, i32, vp]
         L.rg_batch_episode_commands.argtypes = [vp, i32, ctypes.c_uint64, i32, vp, vp]
+        L.rg_batch_phase_timing.argtypes = [vp, i32]
+        L.rg_batch_phase_times.argtypes = [vp, vp, vp]
         _lib = L
     return _lib

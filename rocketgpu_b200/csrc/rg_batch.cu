@@ -112,6 +112,13 @@ struct rg_batch {
     DeviceArray<uint32_t> device_status;          // bit 0: a device command asked for something this build refuses
     DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
     DeviceArray<uint64_t> episode_seen;           // per car slot: latest_touch_tick at the previous episode check
+    // Phase timing (rg_batch_phase_timing): events around the four kernels of every tick, five per tick.
+    bool timing = false;
+    std::vector<cudaEvent_t> events;
+    size_t events_used = 0;
+    ~rg_batch() {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+    }
 };
 
 namespace {
@@ -404,13 +411,27 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
     const int car_blocks = (b->active_car_count + 63) / 64;
+    auto mark = [&] {
+        if (!b->timing) return;
+        if (b->events_used == b->events.size()) {
+            cudaEvent_t e;
+            check(cudaEventCreate(&e), "cudaEventCreate");
+            b->events.push_back(e);
+        }
+        check(cudaEventRecord(b->events[b->events_used++], s), "cudaEventRecord");
+    };
     for (int t = 0; t < ticks; ++t) {
+        mark();
         arena_begin_kernel<<<blocks, threads, 0, s>>>(a, t);
+        mark();
         if (car_blocks) car_pre_kernel<<<car_blocks, 64, 0, s>>>(a, t);
+        mark();
         if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s>>>(a, t);
+        mark();
         // report fields after the last tick, and after every tick of a command stream (reference StepEnvGeneric,
         // env_step.hpp:7174: report_fields = last tick || has_commands)
         arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, (t + 1 == ticks || commands) ? 1 : 0);
+        mark();
     }
     check(cudaGetLastError(), "car tick launch");
 }
@@ -1082,6 +1103,32 @@ RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64
             reinterpret_cast<rg::EnvCommand*>(device_commands), b->env_count, b->max_cars, no_touch_ticks,
             stagger_seed, init);
         check(cudaGetLastError(), "episode_commands_kernel launch");
+    });
+}
+
+RG_API int rg_batch_phase_timing(rg_batch* b, int32_t enable) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        b->timing = enable != 0;
+        b->events_used = 0;
+    });
+}
+
+RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks) {
+    return guard([&] {
+        if (!b || !out_ms) throw std::invalid_argument("null argument");
+        DeviceGuard dg(b->device);
+        for (int k = 0; k < 4; ++k) out_ms[k] = 0.0f;
+        const size_t ticks = b->events_used / 5;
+        if (ticks) check(cudaEventSynchronize(b->events[b->events_used - 1]), "phase timing sync");
+        for (size_t t = 0; t < ticks; ++t)
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0.0f;
+                check(cudaEventElapsedTime(&ms, b->events[5 * t + k], b->events[5 * t + k + 1]), "phase timing");
+                out_ms[k] += ms;
+            }
+        if (out_ticks) *out_ticks = static_cast<int64_t>(ticks);
+        b->events_used = 0;
     });
 }
 

@@ -79,3 +79,42 @@ def test_mesh_tables_match_reference(oracle_available, arena_mesh):
         assert abi.lib().rg_arena_mesh_tables(ctypes.byref(lay), mine.ctypes.data, leaf.ctypes.data, nt) == nt
         assert bytes(mine) == bytes(ref)
         assert (leaf == ref_leaf).all()
+
+
+def _run_mixed(n, ticks, seed, arena_mesh):
+    v, i = arena_mesh
+    rng = np.random.default_rng(seed)
+    counts = rng.choice(np.array([2, 4, 6], np.int32), size=n).astype(np.int32)
+    sim = oracle_ref.OracleSim(n, 6, v, i, kickoff_settled=False)
+    sim.set_env_car_count(counts)
+    sim.reset_to_kickoff(seed)
+    stream = scenarios.ControlStream(n * 6, seed=seed, p_jump=0.1, hold_max=30)
+    for _ in range(ticks // 8):
+        block = np.stack([stream.next() for _ in range(8)]).reshape(-1, 24)
+        sim.step_with_controls(block, 8, n * 6)
+    out = (sim.cars(), sim.balls(), sim.envs(), sim.pads())
+    sim.close()
+    return out
+
+
+def test_native_oracle_build_matches_portable(oracle_available, arena_mesh):
+    """The timed CPU baseline uses an x86-64-v3 build of the reference; with -ffp-contract=off it must step exactly
+    like the portable build the parity tests use."""
+    import ctypes
+    import pytest
+    native = os.path.join(os.path.dirname(oracle_ref.LIB_PATH), "librg_oracle_native.so")
+    if not os.path.exists(native):
+        pytest.skip("native oracle not built")
+    try:
+        ctypes.CDLL(native)
+    except OSError:
+        pytest.skip("native oracle does not load on this host")
+    portable = _run_mixed(48, 240, 5, arena_mesh)
+    saved = (oracle_ref.LIB_PATH, oracle_ref._lib)
+    try:
+        oracle_ref.LIB_PATH, oracle_ref._lib = native, None
+        fast = _run_mixed(48, 240, 5, arena_mesh)
+    finally:
+        oracle_ref.LIB_PATH, oracle_ref._lib = saved
+    for a, b in zip(portable, fast):
+        assert np.array_equal(a, b)
