@@ -330,6 +330,49 @@ typedef struct rg_device_view {
 } rg_device_view;
 RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
 
+/* ---- serving ------------------------------------------------------------------------------------------------------
+ * A serving loop for many RL clients on one GPU. No counterpart in the reference (which steps one BatchSim per call
+ * under a process-wide lock, src/rocketgpu_cuda.cu:2868-2916). The server owns a pool of arena slots sized at open
+ * from an HBM budget; each client owns a contiguous range of slots, created at kickoff as a BatchSim of its own
+ * (its arenas' RNG draws and car ids are numbered within the client), and submits step requests of 1 to 8 ticks
+ * with the controls of every tick. A worker thread runs the pool in rounds of one tick over exactly the arenas whose
+ * request has ticks left, admitting new requests between rounds (continuous batching; policy 1 admits a new batch
+ * only when the previous one has finished: static batching, for comparison). A client's results are bitwise those
+ * of its arenas stepped alone in a BatchSim with the same controls. Status 5 (RG_BUSY): no room for a client now. */
+#define RG_BUSY 5
+typedef struct rg_server rg_server;
+typedef struct rg_server_config {
+    int32_t max_arenas;        /* slot count ceiling (0: the budget alone decides) */
+    int32_t policy;            /* 0 continuous batching, 1 static batching */
+    int64_t hbm_budget_bytes;  /* device bytes the slots may take (0: max_arenas alone decides) */
+} rg_server_config;
+typedef struct rg_server_stats {
+    int64_t capacity, used, slot_bytes, clients, rounds, arena_ticks, completed;
+    double busy_s;             /* device-busy seconds of the rounds */
+} rg_server_stats;
+/* sim: the pool's config (env_count ignored; max_cars_per_env 1..6, kickoff_settled 0). */
+RG_API int rg_server_open(const rg_server_config* server_config, const rg_sim_config* sim,
+                          const rg_arena_layout* layout, int device, rg_server** out);
+/* Stops the worker after the admitted requests finish, drops queued ones, frees everything. */
+RG_API void rg_server_close(rg_server* s);
+/* Creates `arenas` arenas for a client: car_counts[arenas], teams[arenas * max_cars] (null: all blue),
+ * configs[arenas * max_cars] (null: default body), reset to kickoff with kickoff_seed. RG_BUSY when no free range. */
+RG_API int rg_server_client_open(rg_server* s, int32_t arenas, const int32_t* car_counts, const uint8_t* teams,
+                                 const rg_car_config* configs, uint64_t kickoff_seed, int32_t* client);
+/* Waits for the client's admitted request (if any) to finish, drops its queued and unpolled requests, frees its
+ * slots. */
+RG_API int rg_server_client_close(rg_server* s, int32_t client);
+/* Queues a request: `ticks` in [1, 8], host_controls[ticks][arenas * max_cars] (copied during the call). A client's
+ * requests run in submission order. */
+RG_API int rg_server_submit(rg_server* s, int32_t client, int32_t ticks, const rg_car_controls* host_controls,
+                            int64_t* request);
+/* Waits up to wait_ms for the request; *done = 1 once finished, and then the client's car states
+ * [arenas * max_cars], ball states and env states [arenas] after its last tick are copied to the non-null outputs,
+ * *latency_s (if non-null) is submit-to-finish seconds, and the request is released. */
+RG_API int rg_server_poll(rg_server* s, int64_t request, int32_t wait_ms, rg_car_state* cars_out,
+                          rg_ball_state* balls_out, rg_env_state* envs_out, int32_t* done, double* latency_s);
+RG_API int rg_server_get_stats(rg_server* s, rg_server_stats* out);
+
 /* Steps ball-only arenas whose states live in caller-owned device memory, without allocating any device memory.
  * No counterpart in the reference: an addition of this library.
  *

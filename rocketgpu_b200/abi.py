@@ -24,7 +24,8 @@ EXPORTS = [
     "rg_batch_upload_controls", "rg_batch_step_with_device_controls", "rg_batch_set_teams",
     "rg_batch_reset_to_kickoff", "rg_batch_apply_env_commands", "rg_batch_apply_env_commands_device",
     "rg_batch_step_with_device_commands", "rg_batch_episode_commands", "rg_batch_phase_timing",
-    "rg_batch_phase_times",
+    "rg_batch_phase_times", "rg_server_open", "rg_server_close", "rg_server_client_open", "rg_server_client_close",
+    "rg_server_submit", "rg_server_poll", "rg_server_get_stats",
 ]
 
 
@@ -53,6 +54,16 @@ class rg_device_view(ctypes.Structure):
     _fields_ = [("ball_states", ctypes.c_void_p), ("env_states", ctypes.c_void_p),
                 ("env_car_count", ctypes.c_void_p), ("car_states", ctypes.c_void_p),
                 ("boost_pad_states", ctypes.c_void_p), ("controls", ctypes.c_void_p)]
+
+
+class rg_server_config(ctypes.Structure):
+    _fields_ = [("max_arenas", ctypes.c_int32), ("policy", ctypes.c_int32), ("hbm_budget_bytes", ctypes.c_int64)]
+
+
+class rg_server_stats(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_int64), ("used", ctypes.c_int64), ("slot_bytes", ctypes.c_int64),
+                ("clients", ctypes.c_int64), ("rounds", ctypes.c_int64), ("arena_ticks", ctypes.c_int64),
+                ("completed", ctypes.c_int64), ("busy_s", ctypes.c_double)]
 
 
 _lib = None
@@ -106,5 +117,12 @@ def lib():
         L.rg_batch_episode_commands.argtypes = [vp, i32, ctypes.c_uint64, i32, vp, vp]
         L.rg_batch_phase_timing.argtypes = [vp, i32]
         L.rg_batch_phase_times.argtypes = [vp, vp, vp]
+        L.rg_server_open.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.rg_server_close.argtypes = [vp]
+        L.rg_server_client_open.argtypes = [vp, i32, vp, vp, vp, ctypes.c_uint64, vp]
+        L.rg_server_client_close.argtypes = [vp, i32]
+        L.rg_server_submit.argtypes = [vp, i32, i32, vp, vp]
+        L.rg_server_poll.argtypes = [vp, i64, i32, vp, vp, vp, vp, vp]
+        L.rg_server_get_stats.argtypes = [vp, vp]
         _lib = L
     return _lib

@@ -29,6 +29,10 @@ thread_local std::string g_last_error;
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+// A serving pool without room for a client's arenas (status 5, RG_BUSY): retry after other clients close.
+struct ServerBusy : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 
 void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
@@ -48,6 +52,9 @@ int guard(F&& f) {
     } catch (const CudaError& e) {
         g_last_error = std::string("cuda: ") + e.what();
         return 4;
+    } catch (const ServerBusy& e) {
+        g_last_error = std::string("busy: ") + e.what();
+        return 5;
     } catch (const std::exception& e) {
         g_last_error = e.what();
         return 1;
@@ -207,6 +214,15 @@ __global__ void canonicalize_cars_kernel(rg::CarState* cars, int n) {
     rg::car_re_report_fields(c, kept);
 }
 
+// Per-arena tables of a serving pool (rg_server): ticks left in the arena's current request (0: idle this tick), the
+// control row it reads next, its index among its client's arenas and its client's kickoff seed.
+struct SlotTable {
+    int32_t* remaining;
+    int32_t* tick;
+    const int32_t* logical;
+    const uint64_t* seed;
+};
+
 struct CarTickArgs {
     TickArgs base;
     rg::CarState* cars;
@@ -232,7 +248,22 @@ struct CarTickArgs {
     int32_t command_stride;
     rg::CarControls* reset_controls;  // the batch's held controls, cleared by a kickoff reset
     uint32_t* status;
+    // Serving rounds (rg_server): a tick steps only arenas with ticks left, each reading its controls at its own row
+    // and numbering its env and cars as in a batch of its own. Null: every arena steps, as a batch does.
+    SlotTable slots;
 };
+
+// The control row arena e reads this tick: its own position in its request when serving, else the tick's.
+__device__ __forceinline__ size_t control_row(const CarTickArgs& a, int e, int t) {
+    return static_cast<size_t>(a.slots.remaining ? a.slots.tick[e] : t);
+}
+// The index the arena's RNG draws and car ids use (reference env_idx): its index in its client's arenas when serving.
+__device__ __forceinline__ int logical_env(const CarTickArgs& a, int e) {
+    return a.slots.remaining ? a.slots.logical[e] : e;
+}
+__device__ __forceinline__ bool arena_idle(const CarTickArgs& a, int e) {
+    return a.slots.remaining && a.slots.remaining[e] <= 0;
+}
 
 __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e, int t) {
     const int car_base = e * a.max_cars;
@@ -241,13 +272,13 @@ __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e,
     A.wheels = a.wheels + car_base;
     A.cfgs = a.car_cfgs + car_base;
     A.pads = a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr;
-    A.controls = a.controls ? a.controls + static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + car_base
+    A.controls = a.controls ? a.controls + control_row(a, e, t) * static_cast<size_t>(a.control_stride) + car_base
                             : nullptr;
     A.teams = a.teams + car_base;
     A.pairs = a.pair_slots ? a.pairs + static_cast<size_t>(e) * a.pair_slots : nullptr;
     A.count = a.base.env_car_count[e];
     A.max_cars = a.max_cars;
-    A.car_base = car_base;
+    A.car_base = logical_env(a, e) * a.max_cars;  // car ids are car_base + slot + 1
     return A;
 }
 
@@ -291,6 +322,7 @@ __global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
+    if (arena_idle(a, e)) return;
     if (a.commands) {
         const rg::EnvCommand c = a.commands[static_cast<size_t>(t) * static_cast<size_t>(a.command_stride) + e];
         if (rg::env_command_active(c) && !command_refused(c, a.status))
@@ -312,13 +344,15 @@ __global__ void __launch_bounds__(64) car_pre_kernel(CarTickArgs a, int t) {
     if (k >= a.active_car_count) return;
     const int idx = a.active_cars[k];
     const int e = idx / a.max_cars;
+    if (arena_idle(a, e)) return;
     const rg::CarControls& ctrl =
-        a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+        a.controls[control_row(a, e, t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+    const int le = logical_env(a, e);
     rg::RespawnCtx rc;
-    rc.seed = a.base.tc.kickoff_seed;
-    rc.env_idx = e;
+    rc.seed = a.slots.remaining ? a.slots.seed[e] : a.base.tc.kickoff_seed;
+    rc.env_idx = le;
     rc.env_tick = a.base.envs[e].tick;
-    rc.car_id = static_cast<uint32_t>(idx + 1);
+    rc.car_id = static_cast<uint32_t>(le * a.max_cars + (idx - e * a.max_cars) + 1);
     rc.team = a.teams[idx];
     rg::car_tick_pre(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], rc, a.records[idx]);
 }
@@ -330,11 +364,12 @@ __global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
     if (k >= a.active_car_count) return;
     const int idx = a.active_cars[k];
     const int e = idx / a.max_cars;
+    if (arena_idle(a, e)) return;
     const int base = e * a.max_cars;
     const int count = a.base.env_car_count[e];
     if (rg::arena_wheel_reach_near(a.cars + base, a.car_cfgs + base, count)) return;
     const rg::CarControls& ctrl =
-        a.controls[static_cast<size_t>(t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+        a.controls[control_row(a, e, t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
     const uint32_t excluded =
         a.cars[idx].is_demoed ? 0u
                               : rg::wheel_ray_excluded_bodies(a.cars[idx], a.car_cfgs[idx], a.broadphase + e, idx - base,
@@ -349,16 +384,22 @@ __global__ void __launch_bounds__(32) arena_finish_kernel(CarTickArgs a, int t, 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
+    if (arena_idle(a, e)) return;
     rg::BallState b = a.base.balls[e];
     rg::EnvState env = a.base.envs[e];
     rg::BallWorldScratch s = a.base.ball_world[e];
     const int car_base = e * a.max_cars;
+    // serving: report fields after the request's last tick, as a batch reports them after a step's last tick
+    const bool report = a.slots.remaining ? a.slots.remaining[e] == 1 : report_fields != 0;
     rg::arena_tick_finish(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc,
-                          a.base.mesh, arena_cars(a, e, t), a.pad_layout, report_fields != 0, a.records + car_base,
-                          a.snaps[e]);
+                          a.base.mesh, arena_cars(a, e, t), a.pad_layout, report, a.records + car_base, a.snaps[e]);
     a.base.balls[e] = b;
     a.base.envs[e] = env;
     a.base.ball_world[e] = s;
+    if (a.slots.remaining) {
+        --a.slots.remaining[e];
+        ++a.slots.tick[e];
+    }
 }
 
 CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stride) {
@@ -393,6 +434,7 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     a.command_stride = 0;
     a.reset_controls = b->controls.ptr;
     a.status = b->device_status.ptr;
+    a.slots = SlotTable{};
     return a;
 }
 
@@ -437,9 +479,12 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
 }
 
 // reset_to_kickoff for every arena (reference BatchSim::reset_to_kickoff, src/rocketgpu.cpp:2085-2132).
-__global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::CarControls* controls, uint64_t seed) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.base.env_count) return;
+// Arenas [first, first + n) reset; their RNG draws use their index within the range (the whole batch: first = 0).
+__global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::CarControls* controls, uint64_t seed,
+                                     int first, int n) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int e = first + j;
     const int car_base = e * a.max_cars;
     // the reference resets the arena's whole solver scratch (src/rocketgpu.cpp:2107-2111): broadphase history,
     // manifold list and retained car manifolds start over
@@ -449,7 +494,7 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
         a.ball_car[car_base + k].count = 0;
     }
     for (int k = 0; k < a.pair_slots; ++k) a.pairs[static_cast<size_t>(e) * a.pair_slots + k].count = 0;
-    rg::reset_env_to_kickoff(e, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
+    rg::reset_env_to_kickoff(j, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
                              a.car_cfgs + car_base, controls + car_base,
                              a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
                              teams + car_base, a.base.env_car_count[e], a.max_cars, a.base.tc);
@@ -507,7 +552,8 @@ void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
     b->tc.kickoff_seed = seed;  // demolished cars draw their respawn spot from the last kickoff seed
     CarTickArgs a = car_tick_args(b, nullptr, 0);
     a.pads = b->pads.ptr;
-    reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed);
+    reset_kickoff_kernel<<<(b->env_count + 63) / 64, 64, 0, s>>>(a, b->teams.ptr, b->controls.ptr, seed, 0,
+                                                                  b->env_count);
     check(cudaGetLastError(), "reset_kickoff_kernel launch");
 }
 
@@ -1255,3 +1301,5 @@ RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, r
 }
 
 }  // extern "C"
+
+#include "rg_server.cuh"

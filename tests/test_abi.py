@@ -99,3 +99,14 @@ def test_parity_compare_allows_only_nan_payloads():
     e = a.copy()
     e[15] = 1
     assert parity.mismatched_bytes(a, e).tolist() == [15]
+
+
+def test_server_rejects_bad_config_before_any_device_call(arena_mesh):
+    from rocketgpu_b200.server import Server
+    v, i = arena_mesh
+    with pytest.raises(ValueError):
+        Server(v, i)  # neither max_arenas nor an HBM budget
+    with pytest.raises(ValueError):
+        Server(v, i, max_arenas=8, max_cars_per_env=7)
+    with pytest.raises(KeyError):
+        Server(v, i, max_arenas=8, policy="fifo")
