@@ -64,6 +64,7 @@ WORKLOADS = {
              "resets (staggered clocks), seeded held controls, procedural 11k-tri arena, 8 ticks per step, "
              "320-tick settle before warm-up",
     "balls": "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step",
+    "serve": "serving loop (see config.workload)",
 }
 # Algorithmic bytes of one arena_finish_kernel launch (one tick), read + write of the state it owns:
 # per arena ball 288, ball contact state 288, env 44, broadphase history 1,344, 34 pads x 16, tick snapshot 24;
@@ -505,6 +506,118 @@ def parity_summary(record, e2e_hashes, final_a, mixed):
             "mismatched_arenas": int((bad_steps | bad_final).sum())}
 
 
+# ---- serving: many clients through rg_server ----------------------------------------------------------------------
+SERVE_CLIENTS = 64
+SERVE_BUDGET = 60 * 1024 ** 3
+
+
+def serve_clients(seed: int, k: int):
+    """Client k's arenas: log-uniform count in [64, 1024], 55/27/18 mix, first half of each arena's cars blue."""
+    rng = np.random.default_rng(seed * 1000 + k)
+    n = int(np.exp(rng.uniform(np.log(64), np.log(1024))))
+    counts = rng.choice(np.array([2, 4, 6], np.int32), size=n, p=[0.55, 0.27, 0.18]).astype(np.int32)
+    teams = np.zeros(n * MAX_CARS, np.uint8)
+    for e in range(n):
+        teams[e * MAX_CARS + counts[e] // 2: e * MAX_CARS + counts[e]] = 1
+    return counts, teams
+
+
+def run_serve_policy(srv_policy, rate, seconds, seed, v, i):
+    """Poisson step requests (ticks in {1, 4, 8}) at `rate` per second spread over the clients, 1 % of clients closed
+    and reopened per second; returns throughput and latency percentiles."""
+    from tests import scenarios
+    from rocketgpu_b200.server import Busy, Server
+    specs = [serve_clients(seed, k) for k in range(SERVE_CLIENTS)]
+    cap = int(sum(len(c) for c, _ in specs) * 1.3)
+    srv = Server(v, i, max_arenas=cap, hbm_budget_bytes=SERVE_BUDGET, policy=srv_policy, max_cars_per_env=MAX_CARS)
+    rng = np.random.default_rng(seed)
+    clients = []
+    for k, (counts, teams) in enumerate(specs):
+        clients.append([srv.open_client(counts, teams, kickoff_seed=seed + k), len(counts), 0])
+    ctrl_cache = {}
+
+    def controls(n, ticks):
+        key = (n, ticks)
+        if key not in ctrl_cache:
+            st = scenarios.ControlStream(n * MAX_CARS, seed=n * 10 + ticks, p_jump=0.1, hold_max=30)
+            ctrl_cache[key] = np.stack([st.next() for _ in range(ticks)])
+        return ctrl_cache[key]
+
+    outstanding = []
+    lat, done_ticks, refused = [], 0, 0
+    t_start = time.perf_counter()
+    next_arrival = t_start + rng.exponential(1.0 / rate)
+    next_churn = t_start + rng.exponential(1.0 / (0.01 * SERVE_CLIENTS))
+    reopened = 0
+    while True:
+        now = time.perf_counter()
+        if now - t_start >= seconds:
+            break
+        while next_arrival <= now:
+            c = clients[rng.integers(0, SERVE_CLIENTS)]
+            ticks = int(rng.choice([1, 4, 8]))
+            outstanding.append((srv.submit(c[0], controls(c[1], ticks)), c[1] * ticks))
+            next_arrival += rng.exponential(1.0 / rate)
+        if next_churn <= now:
+            k = int(rng.integers(0, SERVE_CLIENTS))
+            counts, teams = serve_clients(seed + 7919 + reopened, k)
+            # closing waits for the client's admitted request and drops its queued ones (polling those then reports
+            # an unknown request, below)
+            srv.close_client(clients[k][0])
+            try:
+                clients[k] = [srv.open_client(counts, teams, kickoff_seed=reopened), len(counts), 0]
+            except Busy:
+                refused += 1
+                clients[k] = [srv.open_client(specs[k][0], specs[k][1], kickoff_seed=reopened), len(specs[k][0]), 0]
+            reopened += 1
+            next_churn += rng.exponential(1.0 / (0.01 * SERVE_CLIENTS))
+        keep = []
+        for req, work in outstanding:
+            try:
+                res = srv.poll(req)
+            except IndexError:
+                continue  # its client was closed before it ran
+            if res is None:
+                keep.append((req, work))
+            else:
+                lat.append(res[0])
+                done_ticks += work
+        outstanding = keep
+        time.sleep(0.0002)
+    elapsed = time.perf_counter() - t_start
+    stats = srv.stats()
+    srv.close()
+    lat_ms = np.array(lat) * 1e3 if lat else np.array([float("nan")])
+    return {"policy": srv_policy, "offered_req_per_s": rate, "completed": len(lat),
+            "throughput_arena_ticks_per_s": done_ticks / elapsed,
+            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+            "p999_ms": float(np.percentile(lat_ms, 99.9)), "rounds": stats["rounds"],
+            "device_busy_frac": stats["busy_s"] / elapsed, "pool_slots": stats["capacity"],
+            "slot_bytes": stats["slot_bytes"], "clients_reopened": reopened, "reopen_refused": refused}
+
+
+def run_serve(args, world, rank, local):
+    import torch
+
+    from rocketgpu_b200 import arena
+    torch.cuda.set_device(local)
+    v, i = arena.generate()
+    out = {}
+    for policy in ("static", "continuous"):
+        out[policy] = run_serve_policy(policy, args.rate, args.serve_seconds, 11 + rank, v, i)
+    cont = out["continuous"]
+    return {
+        "metric": METRIC, "value": cont["throughput_arena_ticks_per_s"] * world, "unit": "arena-ticks/s",
+        "n_gpus": world, "steps": 0, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded clients, Poisson step requests)",
+        "config": {"workload": f"serving: {SERVE_CLIENTS} clients x log-uniform 64..1024 arenas (55/27/18), Poisson "
+                               f"requests at {args.rate:g}/s with ticks in {{1,4,8}}, 1%/s client churn, "
+                               f"{SERVE_BUDGET / 1024 ** 3:.0f} GiB HBM budget, {args.serve_seconds:g} s per policy"},
+        "serving": out,
+        "gpu_launches": None,
+    }
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -532,6 +645,8 @@ def main():
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--arenas", type=int, default=ENVS, help="arenas per GPU (smaller cases for profiling)")
+    ap.add_argument("--rate", type=float, default=1000.0, help="serving: offered step requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving: seconds per policy")
     args = ap.parse_args()
     if args.arenas != ENVS:
         globals()["ENVS"] = args.arenas
@@ -545,7 +660,7 @@ def main():
         line = run_reference(args, world, rank)
     else:
         world, rank, local = dist_setup(args.gpus)
-        line = run_ours(args, world, rank, local)
+        line = run_serve(args, world, rank, local) if args.workload == "serve" else run_ours(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

@@ -304,6 +304,14 @@ RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks);
  * command that was refused (invalid_argument). */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
 
+/* Arenas on different geometries in one batch. The reference takes one geometry per BatchSim (ArenaLayout,
+ * rocketgpu.h:943-959), so a mix of arenas needs one BatchSim per mesh there; here one batch holds up to 255 meshes.
+ * rg_batch_add_mesh uploads another layout's mesh and returns its index (the create-time mesh is 0);
+ * rg_batch_set_arena_meshes sets arena i's mesh to host_mesh_index[i] for i < count (initially every arena is on mesh
+ * 0). An arena's results are those of the same arena in a batch created with its mesh. */
+RG_API int rg_batch_add_mesh(rg_batch* b, const rg_arena_layout* layout, int32_t* mesh_index);
+RG_API int rg_batch_set_arena_meshes(rg_batch* b, const uint8_t* host_mesh_index, size_t count, void* stream);
+
 /* The arena tables rg_batch_create builds from a layout, for inspection: per triangle (caller order) 16 floats
  * a, b, c, normal (Bullet units, uu / 50), the three internal-edge angles and the edge flags (as a float), and the
  * BVH leaf order (caller triangle index of each leaf in the order queries visit them). Host only. Returns the

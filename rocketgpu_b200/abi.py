@@ -25,7 +25,7 @@ EXPORTS = [
     "rg_batch_reset_to_kickoff", "rg_batch_apply_env_commands", "rg_batch_apply_env_commands_device",
     "rg_batch_step_with_device_commands", "rg_batch_episode_commands", "rg_batch_phase_timing",
     "rg_batch_phase_times", "rg_server_open", "rg_server_close", "rg_server_client_open", "rg_server_client_close",
-    "rg_server_submit", "rg_server_poll", "rg_server_get_stats",
+    "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
 ]
 
 
@@ -117,6 +117,8 @@ def lib():
         L.rg_batch_episode_commands.argtypes = [vp, i32, ctypes.c_uint64, i32, vp, vp]
         L.rg_batch_phase_timing.argtypes = [vp, i32]
         L.rg_batch_phase_times.argtypes = [vp, vp, vp]
+        L.rg_batch_add_mesh.argtypes = [vp, vp, vp]
+        L.rg_batch_set_arena_meshes.argtypes = [vp, vp, sz, vp]
         L.rg_server_open.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
         L.rg_server_close.argtypes = [vp]
         L.rg_server_client_open.argtypes = [vp, i32, vp, vp, vp, ctypes.c_uint64, vp]

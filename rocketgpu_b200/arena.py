@@ -194,3 +194,8 @@ def generate(fillet_segments: int = 16, seg_len: float = 384.0, wall_bands: int 
 def generate_dense(fillet_segments: int = 64):
     """The ~40k-triangle variant (64-segment fillets, finer panels)."""
     return generate(fillet_segments=fillet_segments, seg_len=224.0, wall_bands=8, floor_rings=16)
+
+
+def generate_fine(fillet_segments: int = 64):
+    """The contact-heavy stress workload's second geometry: 64-segment fillets and finer panels, ~42k triangles."""
+    return generate(fillet_segments=fillet_segments, seg_len=256.0, wall_bands=6, floor_rings=12)

@@ -74,6 +74,23 @@ class BatchSim:
         self._h = h
         self.config = config
 
+    def add_mesh(self, vertices: np.ndarray, indices: np.ndarray) -> int:
+        """Another arena geometry for this batch; returns its mesh index (the create-time mesh is 0)."""
+        v = np.ascontiguousarray(vertices, np.float32)
+        i = np.ascontiguousarray(indices, np.int32)
+        lay = abi.rg_arena_layout()
+        lay.vertices_uu = v.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        lay.vertex_count = len(v)
+        lay.indices = i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        lay.index_count = len(i)
+        out = ctypes.c_int32()
+        _check(abi.lib().rg_batch_add_mesh(self._h, ctypes.byref(lay), ctypes.byref(out)))
+        return out.value
+
+    def set_arena_meshes(self, mesh_index, stream: int = 0):
+        m = np.ascontiguousarray(mesh_index, np.uint8)
+        _check(abi.lib().rg_batch_set_arena_meshes(self._h, _ptr(m), len(m), stream))
+
     def close(self):
         if getattr(self, "_h", None):
             abi.lib().rg_batch_destroy(self._h)

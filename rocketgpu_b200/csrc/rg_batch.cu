@@ -69,8 +69,14 @@ struct DeviceArray {
     T* ptr = nullptr;
     size_t n = 0;
     void alloc(size_t count) {
+        reset();
         n = count;
         if (count) check(cudaMalloc(&ptr, count * sizeof(T)), "cudaMalloc");
+    }
+    void reset() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
     }
     ~DeviceArray() {
         if (ptr) cudaFree(ptr);
@@ -111,6 +117,11 @@ struct rg_batch {
     bool pads_live = false;
     rg::MeshHost mesh_host;
     rg::MeshDevice mesh;
+    // further geometries (rg_batch_add_mesh): all meshes, the create-time one first, and each arena's mesh index;
+    // the table stays unallocated while the batch has one mesh
+    std::vector<rg::MeshDevice> extra_meshes;
+    DeviceArray<rg::MeshDevice> mesh_table;
+    DeviceArray<uint8_t> mesh_of;
     std::vector<int32_t> host_car_count;
     std::vector<int32_t> host_arena_order, host_active_cars;
     int launch_threads = 32;
@@ -176,7 +187,15 @@ struct TickArgs {
     int32_t env_count;
     rg::TickConfig tc;
     rg::MeshDevice mesh;
+    // arenas on more than one geometry (rg_batch_add_mesh / rg_batch_set_arena_meshes): arena e's mesh is
+    // meshes[mesh_of[e]]; null: every arena on `mesh`
+    const rg::MeshDevice* meshes;
+    const uint8_t* mesh_of;
 };
+
+__device__ __forceinline__ const rg::MeshDevice& arena_mesh(const TickArgs& a, int e) {
+    return a.meshes ? a.meshes[a.mesh_of[e]] : a.mesh;
+}
 
 __global__ void __launch_bounds__(32) tick_kernel(TickArgs a, int ticks) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,8 +203,9 @@ __global__ void __launch_bounds__(32) tick_kernel(TickArgs a, int ticks) {
     rg::BallState b = a.balls[e];
     rg::EnvState env = a.envs[e];
     rg::BallWorldScratch s = a.ball_world[e];
+    const rg::MeshDevice& mesh = arena_mesh(a, e);
     for (int t = 0; t < ticks; ++t) {
-        rg::arena_tick(env, b, s, a.tc, a.mesh);
+        rg::arena_tick(env, b, s, a.tc, mesh);
     }
     a.balls[e] = b;
     a.envs[e] = env;
@@ -374,7 +394,7 @@ __global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
         a.cars[idx].is_demoed ? 0u
                               : rg::wheel_ray_excluded_bodies(a.cars[idx], a.car_cfgs[idx], a.broadphase + e, idx - base,
                                                               count);
-    rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], a.base.mesh,
+    rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], arena_mesh(a.base, e),
                        rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes);
 }
 
@@ -392,7 +412,8 @@ __global__ void __launch_bounds__(32) arena_finish_kernel(CarTickArgs a, int t, 
     // serving: report fields after the request's last tick, as a batch reports them after a step's last tick
     const bool report = a.slots.remaining ? a.slots.remaining[e] == 1 : report_fields != 0;
     rg::arena_tick_finish(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc,
-                          a.base.mesh, arena_cars(a, e, t), a.pad_layout, report, a.records + car_base, a.snaps[e]);
+                          arena_mesh(a.base, e), arena_cars(a, e, t), a.pad_layout, report, a.records + car_base,
+                          a.snaps[e]);
     a.base.balls[e] = b;
     a.base.envs[e] = env;
     a.base.ball_world[e] = s;
@@ -411,6 +432,8 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     a.base.env_count = b->env_count;
     a.base.tc = b->tc;
     a.base.mesh = b->mesh;
+    a.base.meshes = b->mesh_table.ptr;
+    a.base.mesh_of = b->mesh_table.ptr ? b->mesh_of.ptr : nullptr;
     a.cars = b->cars.ptr;
     a.wheels = b->wheels.ptr;
     a.car_cfgs = b->car_cfgs.ptr;
@@ -566,6 +589,8 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
     a.env_count = b->env_count;
     a.tc = b->tc;
     a.mesh = b->mesh;
+    a.meshes = b->mesh_table.ptr;
+    a.mesh_of = b->mesh_table.ptr ? b->mesh_of.ptr : nullptr;
     // One warp per block: an arena is one thread, so 16K arenas are only 512 warps; single-warp blocks spread them
     // over all 148 SMs (128-thread blocks left 20 SMs idle at 16K arenas).
     const int threads = b->launch_threads;
@@ -866,6 +891,7 @@ RG_API void rg_batch_destroy(rg_batch* b) {
     if (!b) return;
     DeviceGuard dg(b->device);
     rg::free_mesh(b->mesh);
+    for (rg::MeshDevice& m : b->extra_meshes) rg::free_mesh(m);
     delete b;
 }
 
@@ -1194,6 +1220,46 @@ RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
     });
 }
 
+RG_API int rg_batch_add_mesh(rg_batch* b, const rg_arena_layout* layout, int32_t* mesh_index) {
+    return guard([&] {
+        if (!b || !layout || !mesh_index) throw std::invalid_argument("null argument");
+        if (b->extra_meshes.size() + 1 >= 255) throw std::out_of_range("a batch holds at most 255 meshes");
+        rg::MeshHost h = rg::build_mesh_host(layout->vertices_uu, layout->vertex_count, layout->indices,
+                                             layout->index_count);
+        DeviceGuard dg(b->device);
+        check(cudaDeviceSynchronize(), "add_mesh");
+        b->extra_meshes.push_back(rg::upload_mesh(h));
+        std::vector<rg::MeshDevice> table;
+        table.push_back(b->mesh);
+        for (const rg::MeshDevice& m : b->extra_meshes) table.push_back(m);
+        b->mesh_table.alloc(table.size());
+        check(cudaMemcpy(b->mesh_table.ptr, table.data(), table.size() * sizeof(rg::MeshDevice), cudaMemcpyHostToDevice),
+              "mesh table");
+        if (!b->mesh_of.ptr) {
+            b->mesh_of.alloc(b->env_count);
+            check(cudaMemset(b->mesh_of.ptr, 0, b->env_count), "arena meshes");
+        }
+        *mesh_index = static_cast<int32_t>(table.size() - 1);
+    });
+}
+
+RG_API int rg_batch_set_arena_meshes(rg_batch* b, const uint8_t* host_mesh_index, size_t count, void* stream) {
+    return guard([&] {
+        if (!b || (!host_mesh_index && count)) throw std::invalid_argument("null argument");
+        if (count > static_cast<size_t>(b->env_count))
+            throw std::out_of_range("set_arena_meshes count exceeds env_count");
+        const size_t meshes = 1 + b->extra_meshes.size();
+        for (size_t i = 0; i < count; ++i)
+            if (host_mesh_index[i] >= meshes) throw std::out_of_range("mesh index out of range (rg_batch_add_mesh)");
+        if (!count) return;
+        if (meshes == 1) return;  // every index is 0: the batch's one mesh
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(b->mesh_of.ptr, host_mesh_index, count, cudaMemcpyHostToDevice, s), "arena meshes");
+        check(cudaStreamSynchronize(s), "arena meshes");
+    });
+}
+
 RG_API int64_t rg_arena_mesh_tables(const rg_arena_layout* layout, float* out_tri16, int32_t* out_leaf_order,
                                     int64_t cap) {
     int64_t n = -1;
@@ -1294,6 +1360,8 @@ RG_API int rg_batch_step_static_scratch(rg_batch* b, rg_ball_state* dev_balls, r
         a.env_count = env_count;
         a.tc = b->tc;
         a.mesh = b->mesh;
+        a.meshes = b->mesh_table.ptr;
+        a.mesh_of = b->mesh_table.ptr ? b->mesh_of.ptr : nullptr;
         const int threads = b->launch_threads;
         tick_kernel<<<(env_count + threads - 1) / threads, threads, 0, s>>>(a, ticks);
         check(cudaGetLastError(), "tick_kernel launch (static scratch)");

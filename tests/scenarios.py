@@ -177,3 +177,37 @@ class EpisodeClock:
         out = np.zeros((n, ENV_COMMAND_BYTES), np.uint8)
         out[reset, 0:3] = 1
         return out
+
+
+def contact_heavy(cars: np.ndarray, balls: np.ndarray, counts: np.ndarray, max_cars: int, seed: int):
+    """The contact-heavy stress start: each arena's ball at a seeded point in the middle of the field with a velocity
+    of up to 6000 uu/s in a uniform random direction, and its cars spawned within 600 uu of the ball (on the floor or
+    in the air), heading toward the ball at up to supersonic speed. `cars` [envs * max_cars] and `balls` [envs] are the kickoff states to start
+    from; returns the states to upload."""
+    rng = np.random.default_rng(seed)
+    n = balls.shape[0]
+    b = balls.copy()
+    bpos = np.stack([rng.uniform(-2500, 2500, n), rng.uniform(-3500, 3500, n), rng.uniform(150, 900, n)], 1)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    bvel = d * rng.uniform(0, 6000, (n, 1))
+    b[:, OFF_POS:OFF_POS + 12] = bpos.astype(np.float32).view(np.uint8).reshape(n, 12)
+    b[:, OFF_VEL:OFF_VEL + 12] = bvel.astype(np.float32).view(np.uint8).reshape(n, 12)
+    c = cars.copy()
+    for e in range(n):
+        for s in range(int(counts[e])):
+            row = e * max_cars + s
+            off = rng.normal(size=3)
+            off /= np.linalg.norm(off)
+            off *= rng.uniform(200, 600)
+            p = bpos[e] + off
+            p[2] = max(17.0, min(p[2], 1200.0))
+            # heading toward the ball give or take 30 degrees, up to supersonic speed
+            yaw = np.arctan2(bpos[e, 1] - p[1], bpos[e, 0] - p[0]) + rng.uniform(-0.5, 0.5)
+            q = _yaw_quat(np.array([yaw]))[0]
+            v = np.array([np.cos(yaw), np.sin(yaw), 0.0]) * rng.uniform(800, 2300)
+            c[row, CAR_POS:CAR_POS + 12] = p.astype(np.float32).view(np.uint8)
+            c[row, CAR_ROT:CAR_ROT + 16] = q.astype(np.float32).view(np.uint8)
+            c[row, CAR_VEL:CAR_VEL + 12] = v.astype(np.float32).view(np.uint8)
+            c[row, CAR_ON_GROUND] = 1 if p[2] <= 17.0 else 0
+    return c, b
