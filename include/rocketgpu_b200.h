@@ -292,6 +292,18 @@ RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls
 RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64_t stagger_seed, int32_t init,
                                      rg_env_command* device_commands, void* stream);
 
+/* How steps launch (no counterpart in the reference, whose tick-loop graph cache is internal, src/rocketgpu_cuda.cu:
+ * 3764-3876): threads per block of the per-arena kernels and of the per-car kernels (32, 64, 128 or 256; defaults
+ * 32 and 64), and use_graphs != 0 to capture each distinct step (same controls and commands pointers, strides and
+ * tick count) into a CUDA graph on first use and replay it after (up to 16 kept; a change of car counts, pads,
+ * kickoff seed, meshes or launch config drops them). Results do not depend on any of these. rocketgpu_b200.autotune
+ * picks them by timing. While phase timing is on, steps launch without graphs. */
+typedef struct rg_launch_config {
+    int32_t arena_threads, car_threads, use_graphs, reserved;
+} rg_launch_config;
+RG_API int rg_batch_set_launch_config(rg_batch* b, const rg_launch_config* config);
+RG_API int rg_batch_get_launch_config(const rg_batch* b, rg_launch_config* config);
+
 /* Per-kernel device time of the stepping path, for profiling (no counterpart in the reference). While enabled, every
  * tick of a car step records CUDA events on the step's stream around its four kernels (arena begin, car tick start,
  * car vehicle update, arena finish). rg_batch_phase_times waits for the last event, returns the device milliseconds

@@ -26,6 +26,7 @@ EXPORTS = [
     "rg_batch_step_with_device_commands", "rg_batch_episode_commands", "rg_batch_phase_timing",
     "rg_batch_phase_times", "rg_server_open", "rg_server_close", "rg_server_client_open", "rg_server_client_close",
     "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
+    "rg_batch_set_launch_config", "rg_batch_get_launch_config",
 ]
 
 
@@ -54,6 +55,11 @@ class rg_device_view(ctypes.Structure):
     _fields_ = [("ball_states", ctypes.c_void_p), ("env_states", ctypes.c_void_p),
                 ("env_car_count", ctypes.c_void_p), ("car_states", ctypes.c_void_p),
                 ("boost_pad_states", ctypes.c_void_p), ("controls", ctypes.c_void_p)]
+
+
+class rg_launch_config(ctypes.Structure):
+    _fields_ = [("arena_threads", ctypes.c_int32), ("car_threads", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class rg_server_config(ctypes.Structure):
@@ -118,6 +124,8 @@ def lib():
         L.rg_batch_phase_timing.argtypes = [vp, i32]
         L.rg_batch_phase_times.argtypes = [vp, vp, vp]
         L.rg_batch_add_mesh.argtypes = [vp, vp, vp]
+        L.rg_batch_set_launch_config.argtypes = [vp, vp]
+        L.rg_batch_get_launch_config.argtypes = [vp, vp]
         L.rg_batch_set_arena_meshes.argtypes = [vp, vp, sz, vp]
         L.rg_server_open.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
         L.rg_server_close.argtypes = [vp]

@@ -124,8 +124,23 @@ struct rg_batch {
     DeviceArray<uint8_t> mesh_of;
     std::vector<int32_t> host_car_count;
     std::vector<int32_t> host_arena_order, host_active_cars;
-    int launch_threads = 32;
+    int launch_threads = 32;      // threads per block of the per-arena kernels
+    int car_threads = 64;         // threads per block of the per-car kernels
     int pair_slots = 0;
+    // CUDA graphs of whole steps (rg_launch_config.use_graphs): one per (controls, stride, commands, stride, ticks),
+    // captured on first use and replayed after; any change to what a step's launches capture (car counts, pads,
+    // kickoff seed, meshes, launch config) moves graph_version on and drops them
+    bool use_graphs = false;
+    uint64_t graph_version = 0;
+    cudaStream_t capture_stream = nullptr;
+    struct StepGraph {
+        const void *controls, *commands;
+        int32_t control_stride, command_stride, ticks;
+        uint64_t version, last_use;
+        cudaGraphExec_t exec;
+    };
+    std::vector<StepGraph> graphs;
+    uint64_t graph_clock = 0;
     DeviceArray<rg::EnvCommand> command_scratch;  // per arena: the host commands of rg_batch_apply_env_commands
     DeviceArray<uint32_t> device_status;          // bit 0: a device command asked for something this build refuses
     DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
@@ -134,8 +149,15 @@ struct rg_batch {
     bool timing = false;
     std::vector<cudaEvent_t> events;
     size_t events_used = 0;
+    void drop_graphs() {
+        for (StepGraph& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        ++graph_version;
+    }
     ~rg_batch() {
         for (cudaEvent_t e : events) cudaEventDestroy(e);
+        drop_graphs();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
     }
 };
 
@@ -197,7 +219,7 @@ __device__ __forceinline__ const rg::MeshDevice& arena_mesh(const TickArgs& a, i
     return a.meshes ? a.meshes[a.mesh_of[e]] : a.mesh;
 }
 
-__global__ void __launch_bounds__(32) tick_kernel(TickArgs a, int ticks) {
+__global__ void __launch_bounds__(256) tick_kernel(TickArgs a, int ticks) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.env_count) return;
     rg::BallState b = a.balls[e];
@@ -338,7 +360,7 @@ __global__ void apply_commands_kernel(CarTickArgs a, const rg::EnvCommand* cmds,
 
 // Tick part 1, one thread per arena in step order: this tick's env command (step_with_device_commands), vehicle
 // order, the ball's tick start, pad timers.
-__global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
+__global__ void __launch_bounds__(256) arena_begin_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
@@ -359,7 +381,7 @@ __global__ void __launch_bounds__(32) arena_begin_kernel(CarTickArgs a, int t) {
 
 // Tick part 2, one thread per active car: the car's tick start (demolition timer and respawn, quantisation, controls,
 // jumps, dodges, boost) and the speed clamp.
-__global__ void __launch_bounds__(64) car_pre_kernel(CarTickArgs a, int t) {
+__global__ void __launch_bounds__(256) car_pre_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.active_car_count) return;
     const int idx = a.active_cars[k];
@@ -379,7 +401,7 @@ __global__ void __launch_bounds__(64) car_pre_kernel(CarTickArgs a, int t) {
 
 // Tick part 3, one thread per active car: the vehicle update (four suspension rays against the arena mesh and the
 // ball, tyres, drive, air control). Arenas whose cars are within wheel reach of each other are left to part 4.
-__global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
+__global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.active_car_count) return;
     const int idx = a.active_cars[k];
@@ -400,7 +422,7 @@ __global__ void __launch_bounds__(64) car_vehicle_kernel(CarTickArgs a, int t) {
 
 // Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
 // each other, wheel pushes on the ball, the world step, post-tick, pads, goal.
-__global__ void __launch_bounds__(32) arena_finish_kernel(CarTickArgs a, int t, int report_fields) {
+__global__ void __launch_bounds__(256) arena_finish_kernel(CarTickArgs a, int t, int report_fields) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
@@ -475,7 +497,8 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     }
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
-    const int car_blocks = (b->active_car_count + 63) / 64;
+    const int ct = b->car_threads;
+    const int car_blocks = (b->active_car_count + ct - 1) / ct;
     auto mark = [&] {
         if (!b->timing) return;
         if (b->events_used == b->events.size()) {
@@ -489,9 +512,9 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
         mark();
         arena_begin_kernel<<<blocks, threads, 0, s>>>(a, t);
         mark();
-        if (car_blocks) car_pre_kernel<<<car_blocks, 64, 0, s>>>(a, t);
+        if (car_blocks) car_pre_kernel<<<car_blocks, ct, 0, s>>>(a, t);
         mark();
-        if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s>>>(a, t);
+        if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s>>>(a, t);
         mark();
         // report fields after the last tick, and after every tick of a command stream (reference StepEnvGeneric,
         // env_step.hpp:7174: report_fields = last tick || has_commands)
@@ -499,6 +522,44 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
         mark();
     }
     check(cudaGetLastError(), "car tick launch");
+}
+
+// A step through the batch's CUDA graphs when they are on (and phase timing is off): the launches of one step
+// with these pointers are captured once and replayed after.
+void step_car_path(rg_batch* b, const rg::CarControls* controls, int stride, int ticks, cudaStream_t s,
+                   const rg::EnvCommand* commands, int command_stride) {
+    if (!b->use_graphs || b->timing) {
+        launch_car_tick(b, controls, stride, ticks, s, commands, command_stride);
+        return;
+    }
+    if (commands && !b->pads_live) b->drop_graphs();  // the step turns pads on, which captured launches see
+    if (commands) b->pads_live = true;
+    rg_batch::StepGraph* hit = nullptr;
+    for (rg_batch::StepGraph& g : b->graphs)
+        if (g.controls == controls && g.commands == commands && g.control_stride == stride &&
+            g.command_stride == command_stride && g.ticks == ticks && g.version == b->graph_version)
+            hit = &g;
+    if (!hit) {
+        if (!b->capture_stream) check(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking), "capture");
+        if (b->graphs.size() >= 16) {
+            auto lru = std::min_element(b->graphs.begin(), b->graphs.end(),
+                                        [](const auto& x, const auto& y) { return x.last_use < y.last_use; });
+            cudaGraphExecDestroy(lru->exec);
+            b->graphs.erase(lru);
+        }
+        check(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+        launch_car_tick(b, controls, stride, ticks, b->capture_stream, commands, command_stride);
+        cudaGraph_t g = nullptr;
+        check(cudaStreamEndCapture(b->capture_stream, &g), "graph capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "graph instantiate");
+        b->graphs.push_back({controls, commands, stride, command_stride, ticks, b->graph_version, 0, exec});
+        hit = &b->graphs.back();
+    }
+    hit->last_use = ++b->graph_clock;
+    check(cudaGraphLaunch(hit->exec, s), "graph launch");
 }
 
 // reset_to_kickoff for every arena (reference BatchSim::reset_to_kickoff, src/rocketgpu.cpp:2085-2132).
@@ -572,6 +633,7 @@ __global__ void episode_commands_kernel(const rg::EnvState* envs, const rg::CarS
 }
 
 void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
+    if (b->tc.kickoff_seed != seed) b->drop_graphs();  // the respawn seed is part of every captured launch
     b->tc.kickoff_seed = seed;  // demolished cars draw their respawn spot from the last kickoff seed
     CarTickArgs a = car_tick_args(b, nullptr, 0);
     a.pads = b->pads.ptr;
@@ -604,6 +666,7 @@ void launch_tick(rg_batch* b, int ticks, cudaStream_t s) {
 // them), and the active car slots of those arenas in that order. The host copies stay in the batch
 // until the caller's stream has finished the upload (set_env_car_count synchronises it).
 void rebuild_step_order(rg_batch* b, cudaStream_t s) {
+    b->drop_graphs();
     std::vector<int32_t>& order = b->host_arena_order;
     order.resize(b->env_count);
     for (int32_t e = 0; e < b->env_count; ++e) order[e] = e;
@@ -1034,7 +1097,10 @@ RG_API int rg_batch_upload_pad_states(rg_batch* b, const rg_boost_pad_state* hos
     return guard([&] {
         upload_array(b, b->pads, host, count, static_cast<size_t>(rg_batch_pad_capacity(b)), "upload_pad_states",
                      stream);
-        if (count) b->pads_live = true;
+        if (count && !b->pads_live) {
+            b->pads_live = true;
+            b->drop_graphs();
+        }
     });
 }
 RG_API int rg_batch_download_pad_states(rg_batch* b, rg_boost_pad_state* host, size_t count, void* stream) {
@@ -1079,7 +1145,7 @@ RG_API int rg_batch_step(rg_batch* b, int32_t ticks, void* stream) {
         if (ticks == 0) return;
         DeviceGuard dg(b->device);
         if (b->pads_live) {
-            launch_car_tick(b, b->controls.ptr, 0, ticks, static_cast<cudaStream_t>(stream));
+            step_car_path(b, b->controls.ptr, 0, ticks, static_cast<cudaStream_t>(stream), nullptr, 0);
         } else {
             launch_tick(b, ticks, static_cast<cudaStream_t>(stream));
         }
@@ -1096,8 +1162,8 @@ RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls
             throw std::invalid_argument("control_stride must be zero or at least the total car capacity");
         if (control_stride < 0) throw std::invalid_argument("control_stride must be zero or at least the car capacity");
         DeviceGuard dg(b->device);
-        launch_car_tick(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
-                        static_cast<cudaStream_t>(stream));
+        step_car_path(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
+                      static_cast<cudaStream_t>(stream), nullptr, 0);
     });
 }
 
@@ -1158,9 +1224,9 @@ RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls
             throw std::invalid_argument("control_stride must be zero or at least the total car capacity");
         if (command_stride < b->env_count) throw std::invalid_argument("env_command_stride must be at least env_count");
         DeviceGuard dg(b->device);
-        launch_car_tick(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
-                        static_cast<cudaStream_t>(stream), reinterpret_cast<const rg::EnvCommand*>(device_commands),
-                        command_stride);
+        step_car_path(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
+                      static_cast<cudaStream_t>(stream), reinterpret_cast<const rg::EnvCommand*>(device_commands),
+                      command_stride);
     });
 }
 
@@ -1175,6 +1241,30 @@ RG_API int rg_batch_episode_commands(rg_batch* b, int32_t no_touch_ticks, uint64
             reinterpret_cast<rg::EnvCommand*>(device_commands), b->env_count, b->max_cars, no_touch_ticks,
             stagger_seed, init);
         check(cudaGetLastError(), "episode_commands_kernel launch");
+    });
+}
+
+RG_API int rg_batch_set_launch_config(rg_batch* b, const rg_launch_config* c) {
+    return guard([&] {
+        if (!b || !c) throw std::invalid_argument("null argument");
+        auto ok = [](int t) { return t == 32 || t == 64 || t == 128 || t == 256; };
+        if (!ok(c->arena_threads) || !ok(c->car_threads))
+            throw std::invalid_argument("threads per block must be 32, 64, 128 or 256");
+        DeviceGuard dg(b->device);
+        b->launch_threads = c->arena_threads;
+        b->car_threads = c->car_threads;
+        b->use_graphs = c->use_graphs != 0;
+        b->drop_graphs();
+    });
+}
+
+RG_API int rg_batch_get_launch_config(const rg_batch* b, rg_launch_config* c) {
+    return guard([&] {
+        if (!b || !c) throw std::invalid_argument("null argument");
+        c->arena_threads = b->launch_threads;
+        c->car_threads = b->car_threads;
+        c->use_graphs = b->use_graphs ? 1 : 0;
+        c->reserved = 0;
     });
 }
 
@@ -1232,6 +1322,7 @@ RG_API int rg_batch_add_mesh(rg_batch* b, const rg_arena_layout* layout, int32_t
         std::vector<rg::MeshDevice> table;
         table.push_back(b->mesh);
         for (const rg::MeshDevice& m : b->extra_meshes) table.push_back(m);
+        b->drop_graphs();
         b->mesh_table.alloc(table.size());
         check(cudaMemcpy(b->mesh_table.ptr, table.data(), table.size() * sizeof(rg::MeshDevice), cudaMemcpyHostToDevice),
               "mesh table");

@@ -124,10 +124,11 @@ void server_launch_round(rg_server* s) {
     a.slots.seed = s->seed.ptr;
     const int threads = b->launch_threads;
     const int blocks = (b->env_count + threads - 1) / threads;
-    const int car_blocks = (b->active_car_count + 63) / 64;
+    const int ct = b->car_threads;
+    const int car_blocks = (b->active_car_count + ct - 1) / ct;
     arena_begin_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
-    if (car_blocks) car_pre_kernel<<<car_blocks, 64, 0, s->stream>>>(a, 0);
-    if (car_blocks) car_vehicle_kernel<<<car_blocks, 64, 0, s->stream>>>(a, 0);
+    if (car_blocks) car_pre_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
+    if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
     arena_finish_kernel<<<blocks, threads, 0, s->stream>>>(a, 0, 0);
     check(cudaGetLastError(), "serving round launch");
 }
