@@ -347,8 +347,20 @@ typedef struct rg_device_view {
     void* car_states;        /* rg_car_state[car_capacity] */
     void* boost_pad_states;  /* rg_boost_pad_state[pad_capacity] */
     void* controls;          /* rg_car_controls[car_capacity] */
+    void* car_configs;       /* rg_car_config[car_capacity] */
+    uint8_t* teams;          /* [car_capacity], 0 blue / 1 orange */
+    void* wheel_runtime;     /* per car slot, 292 B (the reference's WheelRuntimeState layout), read-only */
 } rg_device_view;
 RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
+
+/* State arrays by name, as the reference's Python binding moves them (download_state_array / upload_state_array,
+ * python/rocketgpu_bindings.cpp:958-1000): name is "car_states", "ball_states", "env_states", "boost_pad_states" or
+ * (upload only) "controls"; host holds `count` raw structs. preserve_internal != 0 uploads cars and balls as they
+ * are (the reference's StateUploadMode::PreserveInternal); 0 canonicalises them as rg_batch_upload_car_states /
+ * rg_batch_upload_ball_states do (PublicState). An unknown name is invalid_argument. Both synchronise the stream. */
+RG_API int rg_batch_upload_state_array(rg_batch* b, const char* name, const void* host, size_t count,
+                                       int32_t preserve_internal, void* stream);
+RG_API int rg_batch_download_state_array(rg_batch* b, const char* name, void* host, size_t count, void* stream);
 
 /* ---- serving ------------------------------------------------------------------------------------------------------
  * A serving loop for many RL clients on one GPU. No counterpart in the reference (which steps one BatchSim per call

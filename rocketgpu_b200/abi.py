@@ -26,7 +26,8 @@ EXPORTS = [
     "rg_batch_step_with_device_commands", "rg_batch_episode_commands", "rg_batch_phase_timing",
     "rg_batch_phase_times", "rg_server_open", "rg_server_close", "rg_server_client_open", "rg_server_client_close",
     "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
-    "rg_batch_set_launch_config", "rg_batch_get_launch_config",
+    "rg_batch_set_launch_config", "rg_batch_get_launch_config", "rg_batch_upload_state_array",
+    "rg_batch_download_state_array",
 ]
 
 
@@ -54,7 +55,8 @@ class rg_arena_layout(ctypes.Structure):
 class rg_device_view(ctypes.Structure):
     _fields_ = [("ball_states", ctypes.c_void_p), ("env_states", ctypes.c_void_p),
                 ("env_car_count", ctypes.c_void_p), ("car_states", ctypes.c_void_p),
-                ("boost_pad_states", ctypes.c_void_p), ("controls", ctypes.c_void_p)]
+                ("boost_pad_states", ctypes.c_void_p), ("controls", ctypes.c_void_p),
+                ("car_configs", ctypes.c_void_p), ("teams", ctypes.c_void_p), ("wheel_runtime", ctypes.c_void_p)]
 
 
 class rg_launch_config(ctypes.Structure):
@@ -125,6 +127,8 @@ def lib():
         L.rg_batch_phase_times.argtypes = [vp, vp, vp]
         L.rg_batch_add_mesh.argtypes = [vp, vp, vp]
         L.rg_batch_set_launch_config.argtypes = [vp, vp]
+        L.rg_batch_upload_state_array.argtypes = [vp, ctypes.c_char_p, vp, sz, i32, vp]
+        L.rg_batch_download_state_array.argtypes = [vp, ctypes.c_char_p, vp, sz, vp]
         L.rg_batch_get_launch_config.argtypes = [vp, vp]
         L.rg_batch_set_arena_meshes.argtypes = [vp, vp, sz, vp]
         L.rg_server_open.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(vp)]

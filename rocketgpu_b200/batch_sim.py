@@ -203,5 +203,44 @@ class BatchSim:
     def device_view(self) -> dict:
         v = abi.rg_device_view()
         _check(abi.lib().rg_batch_device_view(self._h, ctypes.byref(v)))
-        return {"ball_states": v.ball_states, "env_states": v.env_states, "env_car_count": v.env_car_count,
-                "car_states": v.car_states, "boost_pad_states": v.boost_pad_states, "controls": v.controls}
+        return {name: getattr(v, name) for name, _ in v._fields_}
+
+    def boost_pad_capacity(self) -> int:
+        return self.pad_capacity()
+
+    def device_arrays(self) -> dict:
+        """Zero-copy views of the device state arrays (reference BatchSim.device_arrays,
+        python/rocketgpu_bindings.cpp:846-898): per array a dict with a CUDA array interface (one record per element,
+        typestr |V<itemsize>), itemsize, count, per_env and the element it indexes. torch.as_tensor / cupy.asarray
+        take the interface; the views stay valid until the batch is closed."""
+        v = self.device_view()
+        envs, cars = self.env_count(), self.car_capacity()
+        per = cars // envs if envs else 0
+        pads = self.pad_capacity()
+        spec = [("car_states", v["car_states"], cars, CAR_BYTES, per, "car slot", False),
+                ("controls", v["controls"], cars, CONTROLS_BYTES, per, "car slot", False),
+                ("car_configs", v["car_configs"], cars, CAR_CONFIG_BYTES, per, "car slot", False),
+                ("teams", v["teams"], cars, 1, per, "car slot", False),
+                ("ball_states", v["ball_states"], envs, BALL_BYTES, 1, "env", False),
+                ("env_states", v["env_states"], envs, ENV_BYTES, 1, "env", False),
+                ("boost_pad_states", v["boost_pad_states"], pads, PAD_BYTES, pads // envs if envs else 0,
+                 "boost pad", False),
+                ("env_car_count", v["env_car_count"], envs, 4, 1, "env", False),
+                ("wheel_runtime", v["wheel_runtime"], cars, 292, per, "car slot", True)]
+        out = {}
+        for name, ptr, count, size, per_env, element, ro in spec:
+            out[name] = {"__cuda_array_interface__": {"data": (int(ptr or 0), ro), "shape": (count,),
+                                                      "typestr": f"|V{size}", "strides": None, "version": 3},
+                         "itemsize": size, "count": count, "per_env": per_env, "element": element}
+        return out
+
+    def upload_state_array(self, name: str, host_ptr: int, count: int, preserve_internal: bool = False,
+                           stream: int = 0):
+        """Raw structs from host memory by array name (reference BatchSim.upload_state_array)."""
+        _check(abi.lib().rg_batch_upload_state_array(self._h, name.encode(), ctypes.c_void_p(host_ptr), count,
+                                                     int(preserve_internal), stream))
+
+    def download_state_array(self, name: str, host_ptr: int, count: int, stream: int = 0):
+        """Raw structs into host memory by array name (reference BatchSim.download_state_array)."""
+        _check(abi.lib().rg_batch_download_state_array(self._h, name.encode(), ctypes.c_void_p(host_ptr), count,
+                                                       stream))

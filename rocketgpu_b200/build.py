@@ -20,7 +20,7 @@ LIB_NAME = "librocketgpu_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 
 CU_SOURCES = ["rg_batch.cu"]
-CPP_SOURCES = ["rg_mesh.cpp"]
+CPP_SOURCES = ["rg_mesh.cpp"]  # py_module.cpp builds separately (build_py_module)
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
@@ -64,7 +64,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_PATH)
+    build_py_module(verbose)
     return LIB_PATH
+
+
+def build_py_module(verbose: bool = False) -> str:
+    """The pybind11 module rocketgpu_py_b200 (csrc/py_module.cpp) over the C ABI, next to the library it links."""
+    import sysconfig
+
+    import pybind11
+    out = os.path.join(LIB_DIR, "rocketgpu_py_b200" + sysconfig.get_config_var("EXT_SUFFIX"))
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I", os.path.join(ROOT, "include"), "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+           os.path.join(CSRC, "py_module.cpp"), "-L", LIB_DIR, "-lrocketgpu_b200", "-Wl,-rpath,$ORIGIN", "-o", out]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return out
 
 
 if __name__ == "__main__":

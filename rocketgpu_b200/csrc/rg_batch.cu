@@ -1385,7 +1385,46 @@ RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out) {
         out->car_states = b->cars.ptr;
         out->boost_pad_states = b->pads.ptr;
         out->controls = b->controls.ptr;
+        out->car_configs = b->car_cfgs.ptr;
+        out->teams = b->teams.ptr;
+        out->wheel_runtime = b->wheels.ptr;
     });
+}
+
+RG_API int rg_batch_upload_state_array(rg_batch* b, const char* name, const void* host, size_t count,
+                                       int32_t preserve_internal, void* stream) {
+    if (!b || !name) return guard([] { throw std::invalid_argument("null argument"); });
+    const std::string n(name);
+    if (n == "car_states" || n == "ball_states") {
+        if (!preserve_internal)
+            return n == "car_states"
+                       ? rg_batch_upload_car_states(b, static_cast<const rg_car_state*>(host), count, stream)
+                       : rg_batch_upload_ball_states(b, static_cast<const rg_ball_state*>(host), count, stream);
+        return guard([&] {
+            if (n == "car_states")
+                upload_array(b, b->cars, static_cast<const rg_car_state*>(host), count,
+                             static_cast<size_t>(rg_batch_car_capacity(b)), "upload_state_array(car_states)", stream);
+            else
+                upload_array(b, b->balls, static_cast<const rg_ball_state*>(host), count,
+                             static_cast<size_t>(b->env_count), "upload_state_array(ball_states)", stream);
+        });
+    }
+    if (n == "env_states") return rg_batch_upload_env_states(b, static_cast<const rg_env_state*>(host), count, stream);
+    if (n == "boost_pad_states")
+        return rg_batch_upload_pad_states(b, static_cast<const rg_boost_pad_state*>(host), count, stream);
+    if (n == "controls") return rg_batch_upload_controls(b, static_cast<const rg_car_controls*>(host), count, stream);
+    return guard([&] { throw std::invalid_argument("unknown state array: " + n); });
+}
+
+RG_API int rg_batch_download_state_array(rg_batch* b, const char* name, void* host, size_t count, void* stream) {
+    if (!b || !name) return guard([] { throw std::invalid_argument("null argument"); });
+    const std::string n(name);
+    if (n == "car_states") return rg_batch_download_car_states(b, static_cast<rg_car_state*>(host), count, stream);
+    if (n == "ball_states") return rg_batch_download_ball_states(b, static_cast<rg_ball_state*>(host), count, stream);
+    if (n == "env_states") return rg_batch_download_env_states(b, static_cast<rg_env_state*>(host), count, stream);
+    if (n == "boost_pad_states")
+        return rg_batch_download_pad_states(b, static_cast<rg_boost_pad_state*>(host), count, stream);
+    return guard([&] { throw std::invalid_argument("unknown state array: " + n); });
 }
 
 }  // extern "C"

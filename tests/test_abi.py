@@ -110,3 +110,31 @@ def test_server_rejects_bad_config_before_any_device_call(arena_mesh):
         Server(v, i, max_arenas=8, max_cars_per_env=7)
     with pytest.raises(KeyError):
         Server(v, i, max_arenas=8, policy="fifo")
+
+
+def test_pybind_module_mirrors_the_reference_binding(arena_mesh):
+    """rocketgpu_py_b200 (pybind11 over the C ABI) exposes the reference's rocketgpu_py.BatchSim method names; config
+    errors surface as the reference's exception types before any device call."""
+    import importlib
+    import sys
+    sys.path.insert(0, abi.os.path.join(abi.HERE, "_lib"))
+    m = importlib.import_module("rocketgpu_py_b200")
+    for name in ("env_count", "car_capacity", "boost_pad_capacity", "device_view", "set_env_car_count", "set_teams",
+                 "set_car_configs", "upload_car_states", "upload_ball_states", "upload_env_states",
+                 "upload_boost_pad_states", "upload_controls", "download_car_states", "download_ball_states",
+                 "download_env_states", "download_boost_pad_states", "upload_state_array", "download_state_array",
+                 "apply_env_commands", "apply_env_commands_device", "step", "step_with_device_controls",
+                 "step_with_device_commands", "reset_to_kickoff", "synchronize"):
+        assert hasattr(m.BatchSim, name), name
+    cfg = m.SimConfig()
+    assert cfg.kickoff_settled == 0 and cfg.max_cars_per_env == 6
+    v, i = arena_mesh
+    layout = m.ArenaLayout()
+    layout.meshes = [m.ArenaMesh(v, i)]
+    cfg.kickoff_settled = 1
+    with pytest.raises(ValueError, match="kickoff_settled"):
+        m.BatchSim(cfg, layout)
+    cfg.kickoff_settled = 0
+    cfg.max_cars_per_env = 7
+    with pytest.raises(ValueError):
+        m.BatchSim(cfg, layout)
