@@ -107,6 +107,7 @@ struct rg_batch {
     DeviceArray<rg::CarCarManifold> car_pairs;   // per arena: max_cars * (max_cars - 1) / 2 retained car-car manifolds
     DeviceArray<rg::CarTickRecord> car_records;  // per car slot: this tick's record of the car's own update
     DeviceArray<rg::ArenaTickSnap> arena_snaps;  // per arena: the ball's velocities at this tick's start
+    DeviceArray<rg::CarStage> car_stages;        // per car slot: its staged part of this tick's world step
     // Step order: arenas sorted by car count (so a warp's arenas take the same loops), and the active car slots of
     // those arenas in that order (one thread each in the per-car kernel). Rebuilt by set_env_car_count.
     DeviceArray<int32_t> arena_order;
@@ -286,6 +287,7 @@ struct CarTickArgs {
     const int32_t* arena_order;
     const int32_t* active_cars;
     int32_t active_car_count;
+    rg::CarStage* stages;
     const rg::EnvCommand* commands;  // step_with_device_commands: tick t's command for arena e at t * stride + e
     int32_t command_stride;
     rg::CarControls* reset_controls;  // the batch's held controls, cleared by a kickoff reset
@@ -416,8 +418,12 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
         a.cars[idx].is_demoed ? 0u
                               : rg::wheel_ray_excluded_bodies(a.cars[idx], a.car_cfgs[idx], a.broadphase + e, idx - base,
                                                               count);
-    rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], arena_mesh(a.base, e),
+    const rg::MeshDevice& mesh = arena_mesh(a.base, e);
+    rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], mesh,
                        rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes);
+    // the car's own part of the world step, while this thread has the car (rg::CarStage)
+    rg::car_stage_compute(a.cars[idx], a.car_cfgs[idx], a.wheels[idx], a.car_world[idx], a.base.tc, mesh, idx - base,
+                          a.stages[idx]);
 }
 
 // Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
@@ -435,7 +441,7 @@ __global__ void __launch_bounds__(256) arena_finish_kernel(CarTickArgs a, int t,
     const bool report = a.slots.remaining ? a.slots.remaining[e] == 1 : report_fields != 0;
     rg::arena_tick_finish(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc,
                           arena_mesh(a.base, e), arena_cars(a, e, t), a.pad_layout, report, a.records + car_base,
-                          a.snaps[e]);
+                          a.snaps[e], a.stages + car_base);
     a.base.balls[e] = b;
     a.base.envs[e] = env;
     a.base.ball_world[e] = s;
@@ -475,6 +481,7 @@ CarTickArgs car_tick_args(rg_batch* b, const rg::CarControls* controls, int stri
     a.arena_order = b->arena_order.ptr;
     a.active_cars = b->active_cars.ptr;
     a.active_car_count = b->active_car_count;
+    a.stages = b->car_stages.ptr;
     a.commands = nullptr;
     a.command_stride = 0;
     a.reset_controls = b->controls.ptr;
@@ -902,6 +909,7 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
                                                       sizeof(rg::CarCarManifold)),
                   "car-car manifolds");
         b->car_records.alloc(cap);
+        b->car_stages.alloc(cap);
         b->arena_snaps.alloc(b->env_count);
         b->command_scratch.alloc(b->env_count);
         b->device_status.alloc(1);

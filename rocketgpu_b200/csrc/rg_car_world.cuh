@@ -214,12 +214,33 @@ struct CarSplitRow {
     int32_t body, tag;
 };
 constexpr int kMaxCarWorldRows = 5 * 8;  // per car: up to 4 mesh contacts and 1 predictive contact
-struct CarWorldRows {
-    CarVelRow vel[kMaxCarWorldRows];
-    CarFricRow fric[kMaxCarWorldRows];
-    CarSplitRow split[kMaxCarWorldRows];
+// Car/world contact rows with room for N of each kind: an arena's rows (N = kMaxCarWorldRows, slot order), or one
+// car's mesh rows staged by the per-car kernel (N = kCarStageRows: the retained manifold holds at most 4 points).
+template <int N>
+struct CarWorldRowsN {
+    static constexpr int kCap = N;
+    CarVelRow vel[N];
+    CarFricRow fric[N];
+    CarSplitRow split[N];
     int nv, nf, ns;
 };
+using CarWorldRows = CarWorldRowsN<kMaxCarWorldRows>;
+constexpr int kCarStageRows = 4;
+using CarStageRows = CarWorldRowsN<kCarStageRows>;
+
+// Appends one car's staged rows to the arena's rows; its friction rows' normal-row indices move with its normal rows.
+// The arena's rows never fill up (at most 6 cars x 4 mesh contacts + 6 predictive contacts < kMaxCarWorldRows), so
+// appending builds exactly the rows the car's query would have appended in place.
+RG_HDI void append_car_rows(CarWorldRows& dst, const CarStageRows& src) {
+    const int base = dst.nv;
+    for (int k = 0; k < src.nv; ++k) dst.vel[dst.nv++] = src.vel[k];
+    for (int k = 0; k < src.nf; ++k) {
+        CarFricRow r = src.fric[k];
+        r.normal_row += base;
+        dst.fric[dst.nf++] = r;
+    }
+    for (int k = 0; k < src.ns; ++k) dst.split[dst.ns++] = src.split[k];
+}
 
 // The car's inverse inertia in uu (reference MakeCarInvInertiaRowsUu, host_validation_and_contact_debug.hpp:86-129),
 // used by the row builders' validity checks.
@@ -246,12 +267,13 @@ RG_HD V3 mul_rows(V3 r0, V3 r1, V3 r2, V3 v) { return V3{dot(r0, v), dot(r1, v),
 // overrides the mesh and predictive callers pass). `ang_bt` / `tang_ang_bt`: inverse world inertia times (r x n) and
 // (r x t); `split_ang_uu`: the uu-inertia term of the split row's validity check. Returns whether a normal row was
 // made.
-RG_HDI bool car_contact_rows(CarWorldRows& rows, int body, int tag, const CarState& c, V3 normal, V3 rel_bt,
+template <class Rows>
+RG_HDI bool car_contact_rows(Rows& rows, int body, int tag, const CarState& c, V3 normal, V3 rel_bt,
                              float distance_bt, V3 ang_bt, V3 tang_ang_bt, V3 tangent, V3 split_ang_uu,
                              float inv_mass, float restitution, float friction, float dt) {
     const float pen_uu = fmax_(0.0f, -distance_bt) * 50.0f;
     // split (position) row
-    if (!(pen_uu <= 0.0f || dt <= 0.0f) && rows.ns < kMaxCarWorldRows) {
+    if (!(pen_uu <= 0.0f || dt <= 0.0f) && rows.ns < Rows::kCap) {
         const V3 rel_uu = rel_bt * 50.0f;
         const float denom = inv_mass + dot(normal, cross(split_ang_uu, rel_uu));
         if (denom > 1e-8f) {
@@ -272,7 +294,7 @@ RG_HDI bool car_contact_rows(CarWorldRows& rows, int body, int tag, const CarSta
         }
     }
     // normal row
-    if (rows.nv >= kMaxCarWorldRows) return false;
+    if (rows.nv >= Rows::kCap) return false;
     const V3 rel_uu = rel_bt * 50.0f;
     const V3 ang_uu = ang_bt * (1.0f / 50.0f);
     const float denom = inv_mass + dot(normal, cross(ang_uu, rel_uu));
@@ -298,7 +320,7 @@ RG_HDI bool car_contact_rows(CarWorldRows& rows, int body, int tag, const CarSta
     v.body = body;
     v.tag = tag;
     // friction row
-    if (!(friction <= 0.0f) && rows.nf < kMaxCarWorldRows) {
+    if (!(friction <= 0.0f) && rows.nf < Rows::kCap) {
         const V3 tang_ang_uu = tang_ang_bt * (1.0f / 50.0f);
         const float fden = inv_mass + dot(tangent, cross(tang_ang_uu, rel_uu));
         if (fden > 1e-8f) {
@@ -350,9 +372,13 @@ struct CarWorldContactResult {
 // The car's contacts with the arena mesh for this tick: refresh the retained manifold, collect candidates from the
 // triangles the box overlaps, merge them into the manifold and emit rows (body index `body`, source tag 100).
 // `listed`: the car/mesh manifold exists in the broadphase list.
-RG_NOINL CarWorldContactResult car_mesh_contacts(CarState& c, const CarConfig& cfg, CarWorldScratch& ws, bool listed,
-                                               const MeshDevice& mesh, const TickConfig& tc, int body,
-                                               CarWorldRows& rows) {
+// The car does not change here: a hit (res.hit) is recorded by the caller (car_record_world_surface(c, true), once
+// for the points the reference records one by one: the record is idempotent), at the place in the tick where the
+// reference's query runs.
+template <class Rows>
+RG_NOINL CarWorldContactResult car_mesh_contacts(const CarState& c, const CarConfig& cfg, CarWorldScratch& ws,
+                                               bool listed, const MeshDevice& mesh, const TickConfig& tc, int body,
+                                               Rows& rows) {
     CarWorldContactResult res;
     res.hit = false;
     res.latest_normal = V3{0.0f, 0.0f, 1.0f};
@@ -488,7 +514,6 @@ RG_NOINL CarWorldContactResult car_mesh_contacts(CarState& c, const CarConfig& c
         const CarMeshPoint& p = ws.pts[k];
         const V3 pwa = car_world_point(f, r, u, pos, p.local_a);
         const V3 rel_bt = pwa - pos;
-        car_record_world_surface(c, true);
         res.hit = true;
         const V3 ang_bt = mul_rows(i0, i1, i2, cross(rel_bt, p.normal));
         const float pen_uu = fmax_(0.0f, -p.distance) * 50.0f;

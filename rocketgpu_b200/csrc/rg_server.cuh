@@ -110,7 +110,8 @@ int64_t server_slot_bytes(int max_cars) {
                               sizeof(rg::EnvCommand) + sizeof(int64_t) + 3 * sizeof(int32_t) + sizeof(uint64_t);
     const int64_t per_car = sizeof(rg::CarState) + sizeof(rg::WheelRuntime) + sizeof(rg::CarConfig) +
                             (1 + kServerMaxTicks) * sizeof(rg::CarControls) + 1 + sizeof(rg::CarWorldScratch) +
-                            sizeof(rg::BallCarScratch) + sizeof(rg::CarTickRecord) + sizeof(int32_t) +
+                            sizeof(rg::BallCarScratch) + sizeof(rg::CarTickRecord) + sizeof(rg::CarStage) +
+                            sizeof(int32_t) +
                             sizeof(uint64_t);
     return per_arena + static_cast<int64_t>(max_cars) * per_car;
 }

@@ -1021,6 +1021,42 @@ RG_HDI bool ball_car_box_overlaps(const BallState& b, const CarState& car, const
              cmax.z < bmin.z);
 }
 
+// ---- a car's part of the world step, staged ------------------------------------------------------------------
+// What one car of an arena contributes to the world step before the arena's shared stages, computed by the per-car
+// kernel right after the car's vehicle update (one thread per car instead of one per arena): the prestep, the car's
+// predictive contact and its query against the arena mesh, with the retained manifold and the rows that query leaves
+// (as if its manifold is listed, which the arena checks later). Exact: these read and write only the car, its wheel
+// record and its car/mesh manifold (not the ball, the other cars or the broadphase), nothing the arena does between
+// the vehicle update and their place in the world step changes what they read (car/car and car/ball contacts touch
+// only the cars' contact bookkeeping), and their effects on the car (the world-surface record, the contact normal)
+// are applied by the arena where the reference makes them. Arenas whose cars are within wheel reach of each other run
+// the whole world step in the arena thread (their vehicle updates do).
+struct CarStage {
+    PreContactCar pre;
+    V3 pred_n;
+    float pred_d;
+    uint32_t pred_hit;  // the car has a predictive contact this tick
+    uint32_t mesh_ran;  // the mesh query ran (the car is neither demolished at the step's start nor just respawned)
+    CarWorldContactResult res;
+    CarWorldScratch ws;  // the car/mesh manifold after the query
+    CarStageRows rows;   // the query's rows, in the order it made them
+};
+
+RG_HDI void car_stage_compute(CarState& car, const CarConfig& cfg, WheelRuntime& w, const CarWorldScratch& ws_in,
+                              const TickConfig& c, const MeshDevice& mesh, int slot, CarStage& st) {
+    const float sub_dt = c.tick_dt;
+    car_world_prestep(car, cfg, w, c, sub_dt, st.pre);
+    st.pred_hit = !st.pre.is_demoed && car_predictive_hit(car, cfg, mesh, sub_dt, st.pred_n, st.pred_d) ? 1u : 0u;
+    st.mesh_ran = !(st.pre.is_demoed || car.just_respawned) ? 1u : 0u;
+    st.rows.nv = st.rows.nf = st.rows.ns = 0;
+    st.res.hit = false;
+    st.res.latest_normal = V3{0.0f, 0.0f, 1.0f};
+    if (st.mesh_ran) {
+        st.ws = ws_in;
+        st.res = car_mesh_contacts(car, cfg, st.ws, true, mesh, c, slot, st.rows);
+    }
+}
+
 // One arena's world step with cars (reference WorldStepSoccar, env_step.hpp:4727-5623, on the path a custom-mesh
 // soccar arena takes): predictive rays, the broadphase's manifold list, the ball's and the cars' arena contacts, the
 // unified velocity and position solves, then integration; car-ball contacts (reference env_step.hpp:5045-5133)
@@ -1028,7 +1064,8 @@ RG_HDI bool ball_car_box_overlaps(const BallState& b, const CarState& car, const
 // manifold list here.
 RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                             BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
-                            PreContactCar* pre, const TickSnap& snap, uint64_t env_tick) {
+                            PreContactCar* pre, const TickSnap& snap, uint64_t env_tick,
+                            const CarStage* stages = nullptr) {
     const int count = A.count;
     const float sub_dt = c.tick_dt;
     const bool vehicle_woke = (b.sleeping & 4u) != 0;
@@ -1036,7 +1073,11 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
     const bool ball_sleeping = ball_resolve_activation(b);
     if (vehicle_woke) b.deactivation_time = 0.0f;
     const V3 ext_delta = ball_sleeping ? V3{0.0f, 0.0f, 0.0f} : V3{0.0f, 0.0f, c.gravity_z * sub_dt};
-    for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, sub_dt, pre[i]);
+    if (stages) {
+        for (int i = 0; i < count; ++i) pre[i] = stages[i].pre;
+    } else {
+        for (int i = 0; i < count; ++i) car_world_prestep(A.cars[i], A.cfgs[i], A.wheels[i], c, sub_dt, pre[i]);
+    }
     const V3 solver_vel_bt = b.vel_bt;
     // where the bodies stand at the step's start, for the ball-hit records (reference record_ball_car_info)
     const V3 hit_ball_pos = b.pos;
@@ -1055,8 +1096,15 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
     if (!(ball_sleeping && !vehicle_woke) && ball_predictive_hit(b, mesh, sub_dt, pred_n[0], pred_d[0])) pred_mask |= 1u;
     for (int i = 0; i + 1 < body_count; ++i) {
         if (pre[i].is_demoed) continue;
-        if (car_predictive_hit(A.cars[i], A.cfgs[i], mesh, sub_dt, pred_n[i + 1], pred_d[i + 1]))
+        if (stages) {
+            if (stages[i].pred_hit) {
+                pred_n[i + 1] = stages[i].pred_n;
+                pred_d[i + 1] = stages[i].pred_d;
+                pred_mask |= 1u << (i + 1);
+            }
+        } else if (car_predictive_hit(A.cars[i], A.cfgs[i], mesh, sub_dt, pred_n[i + 1], pred_d[i + 1])) {
             pred_mask |= 1u << (i + 1);
+        }
     }
     // broadphase proxies and the manifold list (reference BuildBulletManifoldList + SortBulletManifoldListByIsland)
     BpProxy proxies[kBpBodies];
@@ -1178,8 +1226,19 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
             listed = listed || (bp_kind(key) == 2 && bp_body_a(key) == i && bp_static(key) == 0);
         }
         if (!listed && cws[i].count == 0) continue;
-        const CarWorldContactResult res = car_mesh_contacts(car, A.cfgs[i], cws[i], listed, mesh, c, i, cr);
+        CarWorldContactResult res;
+        if (!stages) {
+            res = car_mesh_contacts(car, A.cfgs[i], cws[i], listed, mesh, c, i, cr);
+        } else if (!listed) {
+            cws[i].count = 0;  // what the query does for an unlisted manifold
+            continue;
+        } else {
+            cws[i] = stages[i].ws;
+            append_car_rows(cr, stages[i].rows);
+            res = stages[i].res;
+        }
         if (res.hit) {
+            car_record_world_surface(car, true);
             car.world_contact.has_contact = 1;
             car.world_contact.contact_normal = res.latest_normal;
         }
@@ -1351,7 +1410,7 @@ RG_HDI bool arena_wheel_reach_near(const CarState* cars, const CarConfig* cfgs, 
 RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                               BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
                               const PadLayout& pads_layout, bool report_fields, CarTickRecord* recs,
-                              const ArenaTickSnap& as) {
+                              const ArenaTickSnap& as, const CarStage* stages = nullptr) {
     const int count = A.count;
     int order[8];
     TickSnap snap;
@@ -1363,7 +1422,8 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     }
     snap.ball_start_vel = as.ball_start_vel;
     snap.ball_vel_bt = as.ball_vel_bt;
-    if (arena_wheel_reach_near(A.cars, A.cfgs, count)) {
+    const bool near = arena_wheel_reach_near(A.cars, A.cfgs, count);
+    if (near) {
         // cars within wheel reach of each other: vehicle updates in the game's car order, wheels seeing other cars
         for (int k = 0; k < count; ++k) {
             const int i = order[k];
@@ -1374,7 +1434,7 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     }
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
-    world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick);
+    world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick, near ? nullptr : stages);
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         CarState& car = A.cars[i];
