@@ -8,8 +8,8 @@ arena. Controls come from the seeded generator (throttle, steer, pitch, yaw, rol
 Bernoulli 0.1 / 0.3 / 0.1; each sample held for U{1..30} ticks). An arena resets to kickoff when its ball is scored or
 when no car has touched the ball for 300 ticks; the no-touch clocks start at seeded ages, so resets are spread over the
 ticks. A step is 8 ticks: one BatchSim::step_with_device_commands over a [8, car_capacity] control block resident in
-HBM, whose first tick applies the resets rg_batch_episode_commands chose after the previous step (4 kernels per tick
-plus the episode kernel, 33 launches per step).
+HBM, whose first tick applies the resets rg_batch_episode_commands chose after the previous step (6 kernels per tick
+plus the episode kernel, 49 launches per step).
 
 Steady state: every arena starts from kickoff, so SETTLE_STEPS untimed steps (320 ticks) run first, then W warm-up
 steps; the K timed steps follow. Every pass (the device-timed pass, the end-to-end pass and the CPU baseline / the
@@ -66,16 +66,23 @@ WORKLOADS = {
     "balls": "ball-only arenas, 16384 arenas/GPU, procedural 11k-tri arena, 8 ticks per step",
     "serve": "serving loop (see config.workload)",
 }
-# Algorithmic bytes of one arena_finish_kernel launch (one tick), read + write of the state it owns:
-# per arena ball 288, ball contact state 288, env 44, broadphase history 1,344, 34 pads x 16, tick snapshot 24;
-# per active car its state 880, wheel record 292, car/mesh manifold 208, car/ball manifold 208, tick record 148, and
-# its control row 24 read once; per car pair (n(n-1)/2 of the arena's n cars) its manifold 260.
-FINISH_BYTES_PER_ARENA = 2 * (288 + 288 + 44 + 1344 + 34 * 16) + 24
-FINISH_BYTES_PER_CAR = 2 * (880 + 292 + 208 + 208 + 148) + 24
-FINISH_BYTES_PER_PAIR = 2 * 260
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one arena_finish_kernel launch at 16,384 arenas, from
-# the ncu capture summarised in profiles/ (a 4,096-arena capture scaled by 4); None until captured.
-FINISH_TRAFFIC = None
+# Algorithmic bytes of one launch (one tick) of each kernel of the car path: read + write of the state it owns, as
+# (bytes per arena, per active car, per car pair). Struct sizes: car 880, wheel record 292, car config 120, controls
+# 24, tick record 136, car stage 1,176 (prestep 56, predictive contact 20, proxy 148, car/mesh manifold 176, query
+# rows and result 776), car/mesh manifold 176, car/ball manifold 272, car-pair manifold 260, ball 288, ball contact
+# state 288, env 44, broadphase history 1,376, 34 pads x 16, tick snapshot 24.
+KERNEL_BYTES = {
+    "arena_begin": (2 * (288 + 44 + 34 * 16) + 24 + 16, 0, 0),
+    "car_pre": (0, 2 * (880 + 292) + 120 + 24 + 136, 0),
+    "car_vehicle": (0, 2 * (880 + 292) + 120 + 24 + 288 + 136 + 176 + 1176, 0),
+    "arena_finish": (2 * (288 + 288 + 1344) + 44 + 24, 2 * (880 + 176 + 272) + 120 + 136 + 1176, 2 * 260),
+    "car_post": (0, 2 * 880 + 292 + 56 + 24, 0),
+    "arena_tail": (2 * (288 + 44 + 34 * 16), 2 * 880 + 120, 0),
+}
+KERNEL_NAMES = ("arena_begin", "car_pre", "car_vehicle", "arena_finish", "car_post", "arena_tail")
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the dominant kernel at 16,384 arenas,
+# from the ncu capture summarised in profiles/ (a smaller capture scaled by arenas); None until captured.
+KERNEL_TRAFFIC = {}
 
 
 def peaks():
@@ -394,7 +401,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    phase_ms = (ctypes.c_float * 4)()
+    phase_ms = (ctypes.c_float * 6)()
     phase_ticks = ctypes.c_int64(0)
     if mixed:
         check(lib.rg_batch_phase_times(sim_a._h, phase_ms, ctypes.byref(phase_ticks)))
@@ -453,27 +460,27 @@ def run_ours(args, world, rank, local):
                                 "max": float(np.max(step_ms)), "e2e_p50": float(np.percentile(e2e_ms, 50)),
                                 "e2e_p99": float(np.percentile(e2e_ms, 99))},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps * (TICKS_PER_STEP * 4 + 1) if mixed else args.steps,
+        "gpu_launches": args.steps * (TICKS_PER_STEP * 6 + 1) if mixed else args.steps,
         "clocks": clocks.summary(),
     }
     if mixed:
         cars_total = int(w.counts.sum())
         pairs_total = int((w.counts * (w.counts - 1) // 2).sum())
         ticks = max(1, phase_ticks.value)
-        finish_ms = phase_ms[3] / ticks
-        finish_bytes = (ENVS * FINISH_BYTES_PER_ARENA + cars_total * FINISH_BYTES_PER_CAR +
-                        pairs_total * FINISH_BYTES_PER_PAIR)
-        achieved = finish_bytes / (finish_ms / 1e3) / 1e9
+        per_launch_ms = {name: phase_ms[k] / ticks for k, name in enumerate(KERNEL_NAMES)}
+        top = max(per_launch_ms, key=per_launch_ms.get)
+        pa, pc, pp = KERNEL_BYTES[top]
+        top_bytes = ENVS * pa + cars_total * pc + pairs_total * pp
+        achieved = top_bytes / (per_launch_ms[top] / 1e3) / 1e9
         line["config"]["cars_per_gpu"] = cars_total
         line["roofline"] = {
-            "bound": "hbm", "kernel": "arena_finish_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_source": peak_kind,
-            "traffic": FINISH_TRAFFIC,
-            "algorithmic_bytes_per_launch": finish_bytes, "avg_launch_ms": finish_ms,
-            "note": "the tick is bound by latency and FP32 issue of serial per-arena work, not by HBM; frac is the "
-                    "HBM fraction of the dominant kernel's algorithmic state bytes"}
-        line["kernel_ms_per_step"] = {name: phase_ms[k] / ticks * TICKS_PER_STEP for k, name in
-                                      enumerate(("arena_begin", "car_pre", "car_vehicle", "arena_finish"))}
+            "traffic": KERNEL_TRAFFIC.get(top),
+            "algorithmic_bytes_per_launch": top_bytes, "avg_launch_ms": per_launch_ms[top],
+            "note": "dominant kernel by device time; the tick is bound by latency and FP32 issue of serial per-arena "
+                    "work, not by HBM; frac is the HBM fraction of its algorithmic state bytes"}
+        line["kernel_ms_per_step"] = {name: ms * TICKS_PER_STEP for name, ms in per_launch_ms.items()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         timing, record = cpu_leg(args.workload, args.warmup, args.steps, parity=True)
         line["cpu_baseline"] = timing

@@ -305,10 +305,10 @@ RG_API int rg_batch_set_launch_config(rg_batch* b, const rg_launch_config* confi
 RG_API int rg_batch_get_launch_config(const rg_batch* b, rg_launch_config* config);
 
 /* Per-kernel device time of the stepping path, for profiling (no counterpart in the reference). While enabled, every
- * tick of a car step records CUDA events on the step's stream around its four kernels (arena begin, car tick start,
- * car vehicle update, arena finish). rg_batch_phase_times waits for the last event, returns the device milliseconds
- * of each kernel summed over the ticks since enabling or the previous call (out_ms[4]) and the tick count, and starts
- * a new sum. Enabling or disabling also starts a new sum. */
+ * tick of a car step records CUDA events on the step's stream around its six kernels (arena begin, car tick start,
+ * car vehicle update, arena finish, car post-tick, arena tail). rg_batch_phase_times waits for the last event, returns
+ * the device milliseconds of each kernel summed over the ticks since enabling or the previous call (out_ms[6]) and
+ * the tick count, and starts a new sum. Enabling or disabling also starts a new sum. */
 RG_API int rg_batch_phase_timing(rg_batch* b, int32_t enable);
 RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks);
 

@@ -146,7 +146,7 @@ struct rg_batch {
     DeviceArray<uint32_t> device_status;          // bit 0: a device command asked for something this build refuses
     DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
     DeviceArray<uint64_t> episode_seen;           // per car slot: latest_touch_tick at the previous episode check
-    // Phase timing (rg_batch_phase_timing): events around the four kernels of every tick, five per tick.
+    // Phase timing (rg_batch_phase_timing): events around the six kernels of every tick, seven per tick.
     bool timing = false;
     std::vector<cudaEvent_t> events;
     size_t events_used = 0;
@@ -423,28 +423,53 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
                        rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes);
     // the car's own part of the world step, while this thread has the car (rg::CarStage)
     rg::car_stage_compute(a.cars[idx], a.car_cfgs[idx], a.wheels[idx], a.car_world[idx], a.base.tc, mesh, idx - base,
-                          a.stages[idx]);
+                          a.records[idx].vel_bt, a.records[idx].ang_vel, a.stages[idx]);
 }
 
 // Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
-// each other, wheel pushes on the ball, the world step, post-tick, pads, goal.
-__global__ void __launch_bounds__(256) arena_finish_kernel(CarTickArgs a, int t, int report_fields) {
+// each other, wheel pushes on the ball, the world step's shared stages.
+__global__ void __launch_bounds__(256) arena_finish_kernel(CarTickArgs a, int t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.base.env_count) return;
+    const int e = a.arena_order[k];
+    if (arena_idle(a, e)) return;
+    rg::BallState b = a.base.balls[e];
+    rg::BallWorldScratch s = a.base.ball_world[e];
+    const int car_base = e * a.max_cars;
+    rg::arena_tick_finish(a.base.envs[e], b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base,
+                          a.base.tc, arena_mesh(a.base, e), arena_cars(a, e, t), a.records + car_base, a.snaps[e],
+                          a.stages + car_base);
+    a.base.balls[e] = b;
+    a.base.ball_world[e] = s;
+}
+
+// Tick part 5, one thread per active car: its integration and post-tick.
+__global__ void __launch_bounds__(256) car_post_kernel(CarTickArgs a, int t, int report_fields) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.active_car_count) return;
+    const int idx = a.active_cars[k];
+    const int e = idx / a.max_cars;
+    if (arena_idle(a, e)) return;
+    // serving: report fields after the request's last tick, as a batch reports them after a step's last tick
+    const bool report = a.slots.remaining ? a.slots.remaining[e] == 1 : report_fields != 0;
+    const rg::CarControls& ctrl =
+        a.controls[control_row(a, e, t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
+    rg::car_tick_post(a.cars[idx], a.stages[idx].pre, ctrl, a.wheels[idx], a.base.tc, report, a.car_cfgs[idx],
+                      a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
+                      a.stages[idx].pads);
+}
+
+// Tick part 6, one thread per arena in step order: pads, the driving countdown, extra ball hits, goal and timers.
+__global__ void __launch_bounds__(256) arena_tail_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;
     const int e = a.arena_order[k];
     if (arena_idle(a, e)) return;
     rg::BallState b = a.base.balls[e];
     rg::EnvState env = a.base.envs[e];
-    rg::BallWorldScratch s = a.base.ball_world[e];
-    const int car_base = e * a.max_cars;
-    // serving: report fields after the request's last tick, as a batch reports them after a step's last tick
-    const bool report = a.slots.remaining ? a.slots.remaining[e] == 1 : report_fields != 0;
-    rg::arena_tick_finish(env, b, s, a.broadphase[e], a.car_world + car_base, a.ball_car + car_base, a.base.tc,
-                          arena_mesh(a.base, e), arena_cars(a, e, t), a.pad_layout, report, a.records + car_base,
-                          a.snaps[e], a.stages + car_base);
+    rg::arena_tick_tail(env, b, arena_cars(a, e, t), a.pad_layout, a.base.tc, a.stages + static_cast<size_t>(e) * a.max_cars);
     a.base.balls[e] = b;
     a.base.envs[e] = env;
-    a.base.ball_world[e] = s;
     if (a.slots.remaining) {
         --a.slots.remaining[e];
         ++a.slots.tick[e];
@@ -523,9 +548,13 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
         mark();
         if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s>>>(a, t);
         mark();
+        arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t);
+        mark();
         // report fields after the last tick, and after every tick of a command stream (reference StepEnvGeneric,
         // env_step.hpp:7174: report_fields = last tick || has_commands)
-        arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t, (t + 1 == ticks || commands) ? 1 : 0);
+        if (car_blocks) car_post_kernel<<<car_blocks, ct, 0, s>>>(a, t, (t + 1 == ticks || commands) ? 1 : 0);
+        mark();
+        arena_tail_kernel<<<blocks, threads, 0, s>>>(a, t);
         mark();
     }
     check(cudaGetLastError(), "car tick launch");
@@ -1288,13 +1317,15 @@ RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks) 
     return guard([&] {
         if (!b || !out_ms) throw std::invalid_argument("null argument");
         DeviceGuard dg(b->device);
-        for (int k = 0; k < 4; ++k) out_ms[k] = 0.0f;
-        const size_t ticks = b->events_used / 5;
+        constexpr int kPhases = 6;
+        for (int k = 0; k < kPhases; ++k) out_ms[k] = 0.0f;
+        const size_t ticks = b->events_used / (kPhases + 1);
         if (ticks) check(cudaEventSynchronize(b->events[b->events_used - 1]), "phase timing sync");
         for (size_t t = 0; t < ticks; ++t)
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < kPhases; ++k) {
                 float ms = 0.0f;
-                check(cudaEventElapsedTime(&ms, b->events[5 * t + k], b->events[5 * t + k + 1]), "phase timing");
+                check(cudaEventElapsedTime(&ms, b->events[(kPhases + 1) * t + k], b->events[(kPhases + 1) * t + k + 1]),
+                      "phase timing");
                 out_ms[k] += ms;
             }
         if (out_ticks) *out_ticks = static_cast<int64_t>(ticks);

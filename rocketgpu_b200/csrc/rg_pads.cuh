@@ -158,6 +158,21 @@ RG_HDI uint64_t pad_contacts_for_car(const CarState& c, const CarConfig& cfg, co
     return hits;
 }
 
+// A car's pad contacts for the pads' tail, computed by the car's own thread after its post-tick: the pads whose
+// sweep the car entered this tick, the pads its box overlaps among those and the pad it was touching, and its frame
+// position. Exact ahead of the arena's pad pass: the geometry reads only the car and the pads' fixed sizes; an
+// earlier car's pickup may clear this car's touching pad, which only makes one overlap bit unused.
+struct PadContacts {
+    uint64_t hits, overlap;
+    V3 frame_pos_bt;
+};
+RG_HDI void pad_contacts_stage(const CarState& c, const CarConfig& cfg, const PadState* pads, const PadLayout& L,
+                               const TickConfig& tc, PadContacts& out) {
+    out.hits = out.overlap = 0u;
+    out.frame_pos_bt = V3{0.0f, 0.0f, 0.0f};
+    if (!c.is_demoed) out.hits = pad_contacts_for_car(c, cfg, pads, L, tc, out.overlap, out.frame_pos_bt);
+}
+
 RG_HDI bool pad_eligible(const CarState& c, const TickConfig& tc) {
     return !c.is_demoed && !c.driving_disabled && c.boost < tc.boost_max;
 }
@@ -231,15 +246,26 @@ RG_HDI void pad_sweep_touch_steps(CarState* cars, int car_base, int max_cars, in
 
 // The pads' part of the tick tail (reference BoostPadTouchPassForEnv, :2706-2835, and PostTickBoostPadsForEnv,
 // :2851-2892). `order` lists the car slots in visit order.
+// `staged` (null: computed here) holds car slot i's pad contacts (pad_contacts_stage) at byte offset
+// i * staged_stride.
 RG_NOINL void pads_tail(CarState* cars, int car_base, int max_cars, const CarConfig* cfgs, int count, const int* order,
-                      PadState* pads, const PadLayout& L, const TickConfig& tc) {
+                      PadState* pads, const PadLayout& L, const TickConfig& tc, const PadContacts* staged = nullptr,
+                      size_t staged_stride = sizeof(PadContacts)) {
     if (!tc.enable_boost_pads || tc.frame_frac < 0.0f) return;
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         CarState& c = cars[i];
         uint64_t overlap = 0u, hits = 0u;
         V3 frame_pos_bt{0.0f, 0.0f, 0.0f};
-        if (!c.is_demoed) hits = pad_contacts_for_car(c, cfgs[i], pads, L, tc, overlap, frame_pos_bt);
+        if (staged) {
+            const PadContacts& pc = *reinterpret_cast<const PadContacts*>(
+                reinterpret_cast<const unsigned char*>(staged) + static_cast<size_t>(i) * staged_stride);
+            hits = pc.hits;
+            overlap = pc.overlap;
+            frame_pos_bt = pc.frame_pos_bt;
+        } else if (!c.is_demoed) {
+            hits = pad_contacts_for_car(c, cfgs[i], pads, L, tc, overlap, frame_pos_bt);
+        }
         if ((hits & (hits - 1u)) != 0u) {
             pad_sweep_touch_steps(cars, car_base, max_cars, i, pads, L, tc, hits, overlap);
         } else {

@@ -130,7 +130,9 @@ void server_launch_round(rg_server* s) {
     arena_begin_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
     if (car_blocks) car_pre_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
     if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
-    arena_finish_kernel<<<blocks, threads, 0, s->stream>>>(a, 0, 0);
+    arena_finish_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
+    if (car_blocks) car_post_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0, 0);
+    arena_tail_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
     check(cudaGetLastError(), "serving round launch");
 }
 

@@ -1040,12 +1040,28 @@ struct CarStage {
     CarWorldContactResult res;
     CarWorldScratch ws;  // the car/mesh manifold after the query
     CarStageRows rows;   // the query's rows, in the order it made them
+    BpProxy proxy;       // the car's broadphase proxy (valid = 0 for a car demolished at the step's start)
+    PadContacts pads;    // the car's pad contacts after its post-tick (pad_contacts_stage)
 };
 
+// A car's broadphase proxy: its box now and at the pose this tick's tick-start velocities predict (reference
+// ComputeBulletBodyProxy, arena_geometry.hpp:3873-4035).
+RG_HDI void car_body_proxy(BpProxy& p, const CarState& car, const CarConfig& cfg, V3 vel_bt, V3 ang_vel, float dt) {
+    V3 ax = car.basis_forward, ay = car.basis_right, az = car.basis_up;
+    V3 px = ax, py = ay, pz = az;
+    Q4 unused{};
+    game_integrate_orientation(px, py, pz, unused, ang_vel, dt);
+    car_proxy(p, car.pos_bt, ax, ay, az, px, py, pz, vel_bt, cfg.hitbox_offset * (1.0f / 50.0f), car_box_half_bt(cfg),
+              dt);
+}
+
 RG_HDI void car_stage_compute(CarState& car, const CarConfig& cfg, WheelRuntime& w, const CarWorldScratch& ws_in,
-                              const TickConfig& c, const MeshDevice& mesh, int slot, CarStage& st) {
+                              const TickConfig& c, const MeshDevice& mesh, int slot, V3 start_vel_bt, V3 start_ang_vel,
+                              CarStage& st) {
     const float sub_dt = c.tick_dt;
     car_world_prestep(car, cfg, w, c, sub_dt, st.pre);
+    st.proxy.valid = 0;
+    if (!st.pre.is_demoed) car_body_proxy(st.proxy, car, cfg, start_vel_bt, start_ang_vel, sub_dt);
     st.pred_hit = !st.pre.is_demoed && car_predictive_hit(car, cfg, mesh, sub_dt, st.pred_n, st.pred_d) ? 1u : 0u;
     st.mesh_ran = !(st.pre.is_demoed || car.just_respawned) ? 1u : 0u;
     st.rows.nv = st.rows.nf = st.rows.ns = 0;
@@ -1111,17 +1127,13 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
     ball_proxy(proxies[0], b.pos_bt, snap.ball_vel_bt, c.ball_radius, sub_dt);
     for (int i = 0; i + 1 < body_count; ++i) {
         BpProxy& p = proxies[i + 1];
-        const CarState& car = A.cars[i];
         if (pre[i].is_demoed) {
             p.valid = 0;
-            continue;
+        } else if (stages) {
+            p = stages[i].proxy;
+        } else {
+            car_body_proxy(p, A.cars[i], A.cfgs[i], snap.car_vel_bt[i], snap.car_ang_vel[i], sub_dt);
         }
-        V3 ax = car.basis_forward, ay = car.basis_right, az = car.basis_up;
-        V3 px = ax, py = ay, pz = az;
-        Q4 unused{};
-        game_integrate_orientation(px, py, pz, unused, snap.car_ang_vel[i], sub_dt);
-        car_proxy(p, car.pos_bt, ax, ay, az, px, py, pz, snap.car_vel_bt[i], A.cfgs[i].hitbox_offset * (1.0f / 50.0f),
-                  car_box_half_bt(A.cfgs[i]), sub_dt);
     }
     BpEntry list[kBpMaxEntries];
     const int n_list = bp_build_manifold_list(bp, proxies, body_count, mesh.aabb_min, mesh.aabb_max, pred_mask,
@@ -1324,7 +1336,7 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
                            len2(b.ang_vel) < kBallAngularSleep * kBallAngularSleep;
         b.deactivation_time = below && !ball_sleeping ? b.deactivation_time + sub_dt : 0.0f;
     }
-    for (int i = 0; i < count; ++i) car_world_finish(A.cars[i], pre[i], sub_dt);
+    // each car's integration (car_world_finish) follows in car_tick_post, one thread per car
 }
 
 // The game's extra ball-hit impulses of this tick, as a velocity change of the ball (reference ApplyBallExtraHits,
@@ -1346,14 +1358,19 @@ RG_HDI void apply_ball_extra_hits(BallState& b, CarState* cars, int count, const
     if (any) ball_set_vel_bt(b, v);
 }
 
-// A tick of an arena with cars runs in three parts, so that the cars' own updates can run one thread per car:
-//   arena_tick_begin   (per arena)  the game's vehicle order, the ball's tick start, the pads' timers;
-//   car_tick_vehicle   (per car)    the car's tick start and its vehicle update (suspension rays, tyres, jumps,
-//                                   boost, air control), recording what the world step needs from it;
-//   arena_tick_finish  (per arena)  the wheel pushes on the ball in car order, the world step, post-tick, pads, goal.
-// Reordering is exact: a car's tick start and vehicle update read and write only that car (the ball only through its
-// position, which none of them moves), and the ball's tick start reads no car, so running the cars' parts after the
-// ball's tick start and before any push is applied gives the reference's results bit for bit
+// A tick of an arena with cars runs in six parts, so that each car's own work runs one thread per car:
+//   arena_tick_begin   (per arena)  this tick's env command, the game's vehicle order, the ball's tick start, pad timers;
+//   car_tick_pre       (per car)    the car's tick start (demolition timer and respawn, quantisation, controls, jumps);
+//   vehicle_update + car_stage_compute (per car, arenas whose cars are out of each other's wheel reach)
+//                                   the vehicle update, then the car's prestep, predictive contact, broadphase proxy
+//                                   and mesh contact query (CarStage);
+//   arena_tick_finish  (per arena)  near arenas' vehicle updates in car order, the wheel pushes on the ball in car
+//                                   order, the world step's shared stages (manifold list, car/car, car/ball, ball/mesh
+//                                   contacts, the unified solves, the ball's integration);
+//   car_tick_post      (per car)    the car's integration and post-tick;
+//   arena_tick_tail    (per arena)  pads in car order, the driving countdown, extra ball hits, goal and timers.
+// Reordering is exact: each per-car part reads and writes only that car (the ball only through its position, which
+// none of them moves), and the arena parts keep the reference's order for everything shared
 // (reference StepEnvGeneric, env_step.hpp:7088-7180).
 
 // What the world step needs from one car's tick start and vehicle update.
@@ -1409,8 +1426,7 @@ RG_HDI bool arena_wheel_reach_near(const CarState* cars, const CarConfig* cfgs, 
 
 RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                               BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
-                              const PadLayout& pads_layout, bool report_fields, CarTickRecord* recs,
-                              const ArenaTickSnap& as, const CarStage* stages = nullptr) {
+                              CarTickRecord* recs, const ArenaTickSnap& as, CarStage* stages) {
     const int count = A.count;
     int order[8];
     TickSnap snap;
@@ -1435,21 +1451,39 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
     world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick, near ? nullptr : stages);
-    for (int k = 0; k < count; ++k) {
-        const int i = order[k];
-        CarState& car = A.cars[i];
-        // a car demolished during this world step reports the rotation it had when the step began (reference
-        // StepEnvPostCar, env_step.hpp:6915-6918)
-        if (!pre[i].is_demoed && !car.just_respawned && car.is_demoed) car.rot = pre[i].rot;
-        car_post_tick(car, A.controls[i], c.tick_dt);
-        car_finish_tick(car);
-        if (report_fields) {
-            report_rlbot_fields(car, A.wheels[i], c);
-        } else {
-            advance_rlbot_fields(car, A.wheels[i], c);
-        }
+    for (int i = 0; i < count; ++i) stages[i].pre = pre[i];  // for the car's own finish (car_tick_post)
+}
+
+// Tick part 5, per car: the car's integration, then its post-tick (reference WorldStepFinishCar + StepEnvPostCar,
+// env_step.hpp:6902-6925). Each car reads and writes only itself, so the cars of an arena run in any order.
+RG_HDI void car_tick_post(CarState& car, const PreContactCar& pre, const CarControls& k, const WheelRuntime& w,
+                          const TickConfig& c, bool report_fields, const CarConfig& cfg, const PadState* pads,
+                          const PadLayout& pads_layout, PadContacts& pad_contacts) {
+    car_world_finish(car, pre, c.tick_dt);
+    // a car demolished during this world step reports the rotation it had when the step began (reference
+    // StepEnvPostCar, env_step.hpp:6915-6918)
+    if (!pre.is_demoed && !car.just_respawned && car.is_demoed) car.rot = pre.rot;
+    car_post_tick(car, k, c.tick_dt);
+    car_finish_tick(car);
+    if (report_fields) {
+        report_rlbot_fields(car, w, c);
+    } else {
+        advance_rlbot_fields(car, w, c);
     }
-    if (A.pads) pads_tail(A.cars, A.car_base, A.max_cars, A.cfgs, count, order, A.pads, pads_layout, c);
+    if (pads && c.enable_boost_pads && !(c.frame_frac < 0.0f))
+        pad_contacts_stage(car, cfg, pads, pads_layout, c, pad_contacts);
+}
+
+// Tick part 6, per arena: pads in the game's car order, the driving countdown, the ball's extra hit impulses and the
+// env tail (reference StepEnvTail, env_step.hpp:6968-7046).
+RG_HDI void arena_tick_tail(EnvState& env, BallState& b, const ArenaCars& A, const PadLayout& pads_layout,
+                            const TickConfig& c, const CarStage* stages) {
+    const int count = A.count;
+    int order[8];
+    for (int k = 0; k < count; ++k) order[k] = car_visit_slot(env, k, count);
+    if (A.pads)
+        pads_tail(A.cars, A.car_base, A.max_cars, A.cfgs, count, order, A.pads, pads_layout, c, &stages[0].pads,
+                  sizeof(CarStage));
     for (int k = 0; k < count; ++k) {
         CarState& car = A.cars[order[k]];
         if (!car.is_demoed && car.driving_disabled) --car.driving_disabled;
