@@ -402,7 +402,8 @@ __global__ void __launch_bounds__(256) car_pre_kernel(CarTickArgs a, int t) {
 }
 
 // Tick part 3, one thread per active car: the vehicle update (four suspension rays against the arena mesh and the
-// ball, tyres, drive, air control). Arenas whose cars are within wheel reach of each other are left to part 4.
+// ball, tyres, drive, air control) and the car's staged world-step parts, for cars whose wheels can land on no other
+// car and under whose car no other wheel can land (rg::arena_free_cars); the others are left to part 4.
 __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.active_car_count) return;
@@ -411,7 +412,10 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
     if (arena_idle(a, e)) return;
     const int base = e * a.max_cars;
     const int count = a.base.env_car_count[e];
-    if (rg::arena_wheel_reach_near(a.cars + base, a.car_cfgs + base, count)) return;
+    const bool free =
+        (rg::arena_free_cars(a.cars + base, a.car_cfgs + base, a.broadphase[e], count) >> (idx - base)) & 1u;
+    a.stages[idx].in_car_thread = free ? 1u : 0u;
+    if (!free) return;  // the arena thread updates this car in the game's car order
     const rg::CarControls& ctrl =
         a.controls[control_row(a, e, t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
     const uint32_t excluded =
@@ -426,8 +430,8 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
                           a.records[idx].vel_bt, a.records[idx].ang_vel, a.stages[idx]);
 }
 
-// Tick part 4, one thread per arena in step order: the vehicle updates of arenas whose cars are within wheel reach of
-// each other, wheel pushes on the ball, the world step's shared stages.
+// Tick part 4, one thread per arena in step order: the vehicle updates (and staged parts) of cars whose wheels may
+// land on other cars, in the game's car order; wheel pushes on the ball; the world step's shared stages.
 __global__ void __launch_bounds__(256) arena_finish_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.base.env_count) return;

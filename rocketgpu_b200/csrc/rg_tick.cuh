@@ -1029,8 +1029,8 @@ RG_HDI bool ball_car_box_overlaps(const BallState& b, const CarState& car, const
 // record and its car/mesh manifold (not the ball, the other cars or the broadphase), nothing the arena does between
 // the vehicle update and their place in the world step changes what they read (car/car and car/ball contacts touch
 // only the cars' contact bookkeeping), and their effects on the car (the world-surface record, the contact normal)
-// are applied by the arena where the reference makes them. Arenas whose cars are within wheel reach of each other run
-// the whole world step in the arena thread (their vehicle updates do).
+// are applied by the arena where the reference makes them. A car whose vehicle update must run in the arena's car
+// order (arena_free_cars) has its stage computed by the arena thread after all those updates.
 struct CarStage {
     PreContactCar pre;
     V3 pred_n;
@@ -1042,6 +1042,7 @@ struct CarStage {
     CarStageRows rows;   // the query's rows, in the order it made them
     BpProxy proxy;       // the car's broadphase proxy (valid = 0 for a car demolished at the step's start)
     PadContacts pads;    // the car's pad contacts after its post-tick (pad_contacts_stage)
+    uint32_t in_car_thread;  // this tick's vehicle update and stage ran in the car's own thread (arena_free_cars)
 };
 
 // A car's broadphase proxy: its box now and at the pose this tick's tick-start velocities predict (reference
@@ -1361,12 +1362,14 @@ RG_HDI void apply_ball_extra_hits(BallState& b, CarState* cars, int count, const
 // A tick of an arena with cars runs in six parts, so that each car's own work runs one thread per car:
 //   arena_tick_begin   (per arena)  this tick's env command, the game's vehicle order, the ball's tick start, pad timers;
 //   car_tick_pre       (per car)    the car's tick start (demolition timer and respawn, quantisation, controls, jumps);
-//   vehicle_update + car_stage_compute (per car, arenas whose cars are out of each other's wheel reach)
+//   vehicle_update + car_stage_compute (per car, cars no other car's wheels can reach and whose wheels reach no other
+//                                   car, arena_free_cars)
 //                                   the vehicle update, then the car's prestep, predictive contact, broadphase proxy
 //                                   and mesh contact query (CarStage);
-//   arena_tick_finish  (per arena)  near arenas' vehicle updates in car order, the wheel pushes on the ball in car
-//                                   order, the world step's shared stages (manifold list, car/car, car/ball, ball/mesh
-//                                   contacts, the unified solves, the ball's integration);
+//   arena_tick_finish  (per arena)  the other cars' vehicle updates in car order and their staged parts, the wheel
+//                                   pushes on the ball in car order, the world step's shared stages (manifold list,
+//                                   car/car, car/ball, ball/mesh contacts, the unified solves, the ball's
+//                                   integration);
 //   car_tick_post      (per car)    the car's integration and post-tick;
 //   arena_tick_tail    (per arena)  pads in car order, the driving countdown, extra ball hits, goal and timers.
 // Reordering is exact: each per-car part reads and writes only that car (the ball only through its position, which
@@ -1405,28 +1408,33 @@ RG_HDI void car_tick_pre(CarState& car, const CarControls& k, const CarConfig& c
     r.pushes.count = 0;
 }
 
-// Whether a suspension ray of one of the arena's cars can reach another car this tick: a symmetric bound on the
-// centre distance (each car's hitbox reach plus 4 bt, which covers the wheel's offset and ray length) that every
-// thread of the arena evaluates alike. Wheels on other cars push those cars at once, so such an arena runs its
-// vehicle updates in the game's car order (arena_tick_finish); all others run them one thread per car.
-RG_HDI float car_wheel_reach_bt(const CarConfig& cfg) {
-    return (0.5f * (fabs_(cfg.hitbox_size.x) + fabs_(cfg.hitbox_size.y) + fabs_(cfg.hitbox_size.z)) +
-            fabs_(cfg.hitbox_offset.x) + fabs_(cfg.hitbox_offset.y) + fabs_(cfg.hitbox_offset.z)) *
-               kUuToBt +
-           2.0f;
-}
-RG_HDI bool arena_wheel_reach_near(const CarState* cars, const CarConfig* cfgs, int count) {
-    for (int i = 0; i < count; ++i)
-        for (int j = i + 1; j < count; ++j) {
-            const float lim = car_wheel_reach_bt(cfgs[i]) + car_wheel_reach_bt(cfgs[j]);
-            if (len2(cars[i].pos_bt - cars[j].pos_bt) <= lim * lim) return true;
-        }
-    return false;
+// The cars of an arena whose vehicle update is independent of the other cars': no other car can be under one of its
+// wheel rays (each other car is demolished or excluded for its rays by the sweep-box rule, wheel_ray_excluded_bodies:
+// the reference never tests those) and it is under no other car's rays. Their updates (and their staged world-step
+// parts) run one thread per car; the other cars' updates run in the game's car order in the arena thread, because a
+// wheel that lands on another car pushes that car at once. Every thread of the arena evaluates this alike from the
+// cars' poses after their tick start, which no vehicle update changes.
+RG_HDI uint32_t arena_free_cars(const CarState* cars, const CarConfig* cfgs, const Broadphase& bp, int count) {
+    uint32_t reach[8];
+    uint32_t under = 0u;
+    for (int i = 0; i < count && i < 8; ++i) {
+        reach[i] = 0u;
+        if (cars[i].is_demoed) continue;
+        const uint32_t ex = wheel_ray_excluded_bodies(cars[i], cfgs[i], &bp, i, count);
+        for (int j = 0; j < count && j < 8; ++j)
+            if (j != i && !cars[j].is_demoed && !((ex >> (j + 1)) & 1u)) reach[i] |= 1u << j;
+        under |= reach[i];
+    }
+    uint32_t free = 0u;
+    for (int i = 0; i < count && i < 8; ++i)
+        if (reach[i] == 0u && !((under >> i) & 1u)) free |= 1u << i;
+    return free;
 }
 
 RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,
                               BallCarScratch* bcs, const TickConfig& c, const MeshDevice& mesh, const ArenaCars& A,
                               CarTickRecord* recs, const ArenaTickSnap& as, CarStage* stages) {
+    // stages[i].in_car_thread: car i's vehicle update and staged parts ran in its own thread this tick
     const int count = A.count;
     int order[8];
     TickSnap snap;
@@ -1438,19 +1446,24 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
     }
     snap.ball_start_vel = as.ball_start_vel;
     snap.ball_vel_bt = as.ball_vel_bt;
-    const bool near = arena_wheel_reach_near(A.cars, A.cfgs, count);
-    if (near) {
-        // cars within wheel reach of each other: vehicle updates in the game's car order, wheels seeing other cars
-        for (int k = 0; k < count; ++k) {
-            const int i = order[k];
-            const uint32_t excluded = A.cars[i].is_demoed ? 0u : wheel_ray_excluded_bodies(A.cars[i], A.cfgs[i], &bp, i, count);
-            vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh,
-                           WheelOthers{A.cars, A.cfgs, count, i, excluded}, recs[i].pushes);
-        }
+    // cars whose wheels may land on other cars: vehicle updates in the game's car order, wheels seeing other cars,
+    // then their staged world-step parts (after every update: a later car's wheel may push an earlier one)
+    uint32_t left = 0u;
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        if (stages[i].in_car_thread) continue;
+        left |= 1u << i;
+        const uint32_t excluded = A.cars[i].is_demoed ? 0u : wheel_ray_excluded_bodies(A.cars[i], A.cfgs[i], &bp, i, count);
+        vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh,
+                       WheelOthers{A.cars, A.cfgs, count, i, excluded}, recs[i].pushes);
     }
+    for (int i = 0; i < count; ++i)
+        if ((left >> i) & 1u)
+            car_stage_compute(A.cars[i], A.cfgs[i], A.wheels[i], cws[i], c, mesh, i, recs[i].vel_bt, recs[i].ang_vel,
+                              stages[i]);
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
-    world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick, near ? nullptr : stages);
+    world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick, stages);
     for (int i = 0; i < count; ++i) stages[i].pre = pre[i];  // for the car's own finish (car_tick_post)
 }
 

@@ -270,7 +270,7 @@ RG_HDI bool wheel_ray_vs_ball(V3 src_bt, V3 dir, float max_len, const BallState&
     return true;
 }
 
-// The other cars of the arena a wheel ray may land on (null `cars`: none within reach, see arena_wheel_reach_near),
+// The other cars of the arena a wheel ray may land on (null `cars`: none can be reached, see arena_free_cars),
 // and the bodies (bit 0 the ball, bit i + 1 car slot i) the car's rays skip this tick (wheel_ray_excluded_bodies).
 struct WheelOthers {
     CarState* cars;
