@@ -353,6 +353,17 @@ typedef struct rg_device_view {
 } rg_device_view;
 RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out);
 
+/* The internal state blob (reference BatchSim internal_state_layout / download_internal_state /
+ * upload_internal_state, python/rocketgpu_bindings.cpp:1002-1060): the device state a batch keeps beyond the public
+ * structs, as consecutive named sections (this build's own layout): wheel_runtime, ball_world, broadphase,
+ * car_world, ball_car, car_pairs (the persistent contact state) and car_stages (the last tick's per-car stages, for
+ * inspection). rg_batch_internal_state_layout gives section `index`'s name and bytes (out_of_range past the last);
+ * the blob is their concatenation. Download then upload restores a batch's internal state exactly (with the public
+ * arrays, a whole snapshot); both synchronise the stream. */
+RG_API int rg_batch_internal_state_layout(rg_batch* b, int32_t index, const char** name, int64_t* bytes);
+RG_API int rg_batch_download_internal_state(rg_batch* b, void* host, void* stream);
+RG_API int rg_batch_upload_internal_state(rg_batch* b, const void* host, void* stream);
+
 /* State arrays by name, as the reference's Python binding moves them (download_state_array / upload_state_array,
  * python/rocketgpu_bindings.cpp:958-1000): name is "car_states", "ball_states", "env_states", "boost_pad_states" or
  * (upload only) "controls"; host holds `count` raw structs. preserve_internal != 0 uploads cars and balls as they

@@ -27,7 +27,8 @@ EXPORTS = [
     "rg_batch_phase_times", "rg_server_open", "rg_server_close", "rg_server_client_open", "rg_server_client_close",
     "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
     "rg_batch_set_launch_config", "rg_batch_get_launch_config", "rg_batch_upload_state_array",
-    "rg_batch_download_state_array",
+    "rg_batch_download_state_array", "rg_batch_internal_state_layout", "rg_batch_download_internal_state",
+    "rg_batch_upload_internal_state",
 ]
 
 
@@ -127,6 +128,9 @@ def lib():
         L.rg_batch_phase_times.argtypes = [vp, vp, vp]
         L.rg_batch_add_mesh.argtypes = [vp, vp, vp]
         L.rg_batch_set_launch_config.argtypes = [vp, vp]
+        L.rg_batch_internal_state_layout.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(i64)]
+        L.rg_batch_download_internal_state.argtypes = [vp, vp, vp]
+        L.rg_batch_upload_internal_state.argtypes = [vp, vp, vp]
         L.rg_batch_upload_state_array.argtypes = [vp, ctypes.c_char_p, vp, sz, i32, vp]
         L.rg_batch_download_state_array.argtypes = [vp, ctypes.c_char_p, vp, sz, vp]
         L.rg_batch_get_launch_config.argtypes = [vp, vp]

@@ -234,6 +234,27 @@ class BatchSim:
                          "itemsize": size, "count": count, "per_env": per_env, "element": element}
         return out
 
+    def internal_state_layout(self) -> list:
+        """[(section name, bytes)] of the internal state blob (reference BatchSim.internal_state_layout)."""
+        out, k = [], 0
+        while True:
+            name, size = ctypes.c_char_p(), ctypes.c_int64()
+            if abi.lib().rg_batch_internal_state_layout(self._h, k, ctypes.byref(name), ctypes.byref(size)) != 0:
+                return out
+            out.append((name.value.decode(), size.value))
+            k += 1
+
+    def download_internal_state(self, stream: int = 0) -> np.ndarray:
+        total = sum(b for _, b in self.internal_state_layout())
+        out = np.zeros(total, np.uint8)
+        _check(abi.lib().rg_batch_download_internal_state(self._h, _ptr(out), stream))
+        return out
+
+    def upload_internal_state(self, blob: np.ndarray, stream: int = 0):
+        b = np.ascontiguousarray(blob, np.uint8)
+        assert b.size == sum(n for _, n in self.internal_state_layout())
+        _check(abi.lib().rg_batch_upload_internal_state(self._h, _ptr(b), stream))
+
     def upload_state_array(self, name: str, host_ptr: int, count: int, preserve_internal: bool = False,
                            stream: int = 0):
         """Raw structs from host memory by array name (reference BatchSim.upload_state_array)."""

@@ -99,6 +99,22 @@ class BatchSim {
         check(rg_batch_download_state_array(b_, name.c_str(), reinterpret_cast<void*>(host_ptr), count,
                                             stream_of(s)));
     }
+    py::list internal_state_layout() const {
+        py::list out;
+        for (int32_t i = 0;; ++i) {
+            const char* name = nullptr;
+            int64_t bytes = 0;
+            if (rg_batch_internal_state_layout(b_, i, &name, &bytes) != 0) break;
+            out.append(py::make_tuple(std::string(name), static_cast<size_t>(bytes)));
+        }
+        return out;
+    }
+    void download_internal_state(uintptr_t host_ptr, uintptr_t s) {
+        check(rg_batch_download_internal_state(b_, reinterpret_cast<void*>(host_ptr), stream_of(s)));
+    }
+    void upload_internal_state(uintptr_t host_ptr, uintptr_t s) {
+        check(rg_batch_upload_internal_state(b_, reinterpret_cast<const void*>(host_ptr), stream_of(s)));
+    }
     void upload_controls(const py::buffer& controls, uintptr_t s) {
         auto c = structs(controls, sizeof(rg_car_controls), "upload_controls");
         check(rg_batch_upload_controls(b_, static_cast<const rg_car_controls*>(c.first), c.second, stream_of(s)));
@@ -231,6 +247,9 @@ PYBIND11_MODULE(rocketgpu_py_b200, m) {
              py::arg("count"), py::arg("preserve_internal") = false, py::arg("stream") = 0)
         .def("download_state_array", &BatchSim::download_state_array, py::arg("name"), py::arg("host_ptr"),
              py::arg("count"), py::arg("stream") = 0)
+        .def("internal_state_layout", &BatchSim::internal_state_layout)
+        .def("download_internal_state", &BatchSim::download_internal_state, py::arg("host_ptr"), py::arg("stream") = 0)
+        .def("upload_internal_state", &BatchSim::upload_internal_state, py::arg("host_ptr"), py::arg("stream") = 0)
         .def("apply_env_commands", &BatchSim::apply_env_commands, py::arg("commands"), py::arg("stream") = 0)
         .def("apply_env_commands_device", &BatchSim::apply_env_commands_device, py::arg("device_commands"),
              py::arg("count"), py::arg("stream") = 0)

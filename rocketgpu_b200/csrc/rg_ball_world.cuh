@@ -575,7 +575,7 @@ RG_HDI void mesh_query_box(const MeshDevice& m, V3 lo, V3 hi, F&& visit) {
     if (small) {
         int cell[3];
         for (int a = 0; a < 3; ++a) {
-            int ci = static_cast<int>(floorf(l3[a] / kQueryCellBt));
+            int ci = x86_f2i(floorf(l3[a] / kQueryCellBt));
             ci = ci < 0 ? 0 : (ci >= m.grid_dims[a] ? m.grid_dims[a] - 1 : ci);
             cell[a] = ci;
         }

@@ -1434,6 +1434,71 @@ RG_API int rg_batch_device_view(rg_batch* b, rg_device_view* out) {
     });
 }
 
+}  // extern "C"
+
+namespace {
+// The internal state blob: named sections of per-arena / per-car device state beyond the public structs (reference
+// BatchSim internal_state_layout / download_internal_state / upload_internal_state, python/rocketgpu_bindings.cpp:
+// 1002-1060, with this build's own sections).
+struct InternalSection {
+    const char* name;
+    void* ptr;
+    size_t bytes;
+};
+std::vector<InternalSection> internal_sections(rg_batch* b) {
+    const size_t env = static_cast<size_t>(b->env_count), cap = env * static_cast<size_t>(b->max_cars);
+    return {
+        {"wheel_runtime", b->wheels.ptr, cap * sizeof(rg::WheelRuntime)},
+        {"ball_world", b->ball_world.ptr, env * sizeof(rg::BallWorldScratch)},
+        {"broadphase", b->broadphase.ptr, env * sizeof(rg::Broadphase)},
+        {"car_world", b->car_world.ptr, cap * sizeof(rg::CarWorldScratch)},
+        {"ball_car", b->ball_car.ptr, cap * sizeof(rg::BallCarScratch)},
+        {"car_pairs", b->car_pairs.ptr, env * static_cast<size_t>(b->pair_slots) * sizeof(rg::CarCarManifold)},
+        {"car_stages", b->car_stages.ptr, cap * sizeof(rg::CarStage)},
+    };
+}
+}  // namespace
+
+extern "C" {
+
+RG_API int rg_batch_internal_state_layout(rg_batch* b, int32_t index, const char** name, int64_t* bytes) {
+    return guard([&] {
+        if (!b || !name || !bytes) throw std::invalid_argument("null argument");
+        const auto secs = internal_sections(b);
+        if (index < 0 || index >= static_cast<int32_t>(secs.size())) throw std::out_of_range("section index");
+        *name = secs[index].name;
+        *bytes = static_cast<int64_t>(secs[index].bytes);
+    });
+}
+
+RG_API int rg_batch_download_internal_state(rg_batch* b, void* host, void* stream) {
+    return guard([&] {
+        if (!b || !host) throw std::invalid_argument("null argument");
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        unsigned char* out = static_cast<unsigned char*>(host);
+        for (const InternalSection& sec : internal_sections(b)) {
+            if (sec.bytes) check(cudaMemcpyAsync(out, sec.ptr, sec.bytes, cudaMemcpyDeviceToHost, s), sec.name);
+            out += sec.bytes;
+        }
+        check(cudaStreamSynchronize(s), "download_internal_state");
+    });
+}
+
+RG_API int rg_batch_upload_internal_state(rg_batch* b, const void* host, void* stream) {
+    return guard([&] {
+        if (!b || !host) throw std::invalid_argument("null argument");
+        DeviceGuard dg(b->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const unsigned char* in = static_cast<const unsigned char*>(host);
+        for (const InternalSection& sec : internal_sections(b)) {
+            if (sec.bytes) check(cudaMemcpyAsync(sec.ptr, in, sec.bytes, cudaMemcpyHostToDevice, s), sec.name);
+            in += sec.bytes;
+        }
+        check(cudaStreamSynchronize(s), "upload_internal_state");
+    });
+}
+
 RG_API int rg_batch_upload_state_array(rg_batch* b, const char* name, const void* host, size_t count,
                                        int32_t preserve_internal, void* stream) {
     if (!b || !name) return guard([] { throw std::invalid_argument("null argument"); });

@@ -271,7 +271,7 @@ RG_HDI float ue3_rotator_sin(int a) { return ue3_sin_tab((a >> 2) & 16383); }
 struct Ue3Rotator {
     int pitch, yaw, roll;
 };
-RG_HDI int ue3_round(float v) { return static_cast<int>(rintf(v + v + 0.5f)) >> 1; }
+RG_HDI int ue3_round(float v) { return x86_f2i(rintf(v + v + 0.5f)) >> 1; }
 // reference Ue3QuatToRotator (math.hpp:1492-1512)
 RG_HDI Ue3Rotator ue3_quat_to_rotator(Q4 q) {
     const float x2 = q.x + q.x, y2 = q.y + q.y, z2 = q.z + q.z;
@@ -532,7 +532,7 @@ RG_HDI float quantize_axis(float x) {
     const float c = clamp1(x);
     const float y = c < 0.0f ? fmax_(c * 128.0f, -128.0f) : fmin_(c * 127.0f, 127.0f);
     const float w = ((y + 128.0f) + (y + 128.0f)) + 0.5f;
-    const int byte = (static_cast<int>(rintf(w)) >> 1) & 0xFF;
+    const int byte = (x86_f2i(rintf(w)) >> 1) & 0xFF;
     const float s = static_cast<float>(byte) - 128.0f;
     constexpr float kInv127 = 1.0f / 127.0f;
     const float q = s * kInv127;
@@ -576,11 +576,11 @@ RG_HDI void cal_internal_timers_from_set_state(CarState& c, const TickConfig& tc
     const float dt = tc.tick_dt;
     c.internal_jump_time = (c.is_jumping || c.has_jumped) ? c.jump_time : 0.0f;
     const float flip_ticks = rintf(c.flip_time / dt);
-    const int m = flip_ticks >= 0.0f ? static_cast<int>(fmin_(flip_ticks, 1.0e6f)) : 0;
+    const int m = flip_ticks >= 0.0f ? x86_f2i(fmin_(flip_ticks, 1.0e6f)) : 0;
     if (c.is_flipping) {
         c.internal_flip_time = cal_accumulated_ticks(m > 1 ? m - 1 : 0, dt);
     } else if (c.has_flipped) {
-        c.internal_flip_time = cal_accumulated_ticks(m + static_cast<int>(rintf(tc.flip_torque_time / dt)), dt);
+        c.internal_flip_time = cal_accumulated_ticks(m + x86_f2i(rintf(tc.flip_torque_time / dt)), dt);
     } else {
         c.internal_flip_time = c.flip_time;
     }
@@ -713,7 +713,7 @@ RG_HDI float cal_flip_restart_time_on_ground(const CarState& c, const TickConfig
     if (c.is_flipping) return 0.0f;
     if (!c.has_flipped) return c.internal_flip_time;
     if (c.internal_flip_time < tc.flip_torque_time) return 0.0f;
-    int k = static_cast<int>(rintf(c.internal_flip_time / dt)) - static_cast<int>(rintf(tc.flip_torque_time / dt));
+    int k = x86_f2i(rintf(c.internal_flip_time / dt)) - x86_f2i(rintf(tc.flip_torque_time / dt));
     if (k < 1) k = 1;
     if (k > 64) return static_cast<float>(k) * dt;
     float t = 0.0f;

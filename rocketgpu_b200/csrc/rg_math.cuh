@@ -58,6 +58,17 @@ RG_HD V3 vmax(V3 a, V3 b) { return V3{fmax_(a.x, b.x), fmax_(a.y, b.y), fmax_(a.
 RG_HD float div50(float x) { return x / 50.0f; }
 RG_HD V3 uu_to_bt_div(V3 v) { return V3{div50(v.x), div50(v.y), div50(v.z)}; }
 
+// Float-to-integer conversions as the reference's x86 build performs them (cvttss2si / cvttsd2si): truncation toward
+// zero, and the "integer indefinite" INT32_MIN for NaN and for values outside int32. CUDA's conversions saturate and
+// turn NaN into 0, so the tick converts through these wherever a value may be NaN or out of range (a car whose state
+// went NaN, a huge angle); in range they are plain truncations on both.
+RG_HD int32_t x86_f2i(float x) {
+    return (x >= -2147483648.0f && x < 2147483648.0f) ? static_cast<int32_t>(x) : INT32_MIN;
+}
+RG_HD int32_t x86_d2i(double x) {
+    return (x > -2147483649.0 && x < 2147483648.0) ? static_cast<int32_t>(x) : INT32_MIN;
+}
+
 // Index of the lowest set bit (x != 0).
 RG_HD int ctz32(uint32_t x) {
 #if defined(__CUDA_ARCH__)
@@ -111,7 +122,7 @@ RG_HDI double ucrt_cos_poly(double r) {
     return fma(p, r2 * r2, base);
 }
 RG_HDI double ucrt_reduce(double a, int* quadrant) {
-    const int n = static_cast<int>(fma(a, 0x1.45f306dc9c883p-1, 0.5));
+    const int n = x86_d2i(fma(a, 0x1.45f306dc9c883p-1, 0.5));
     const double nd = static_cast<double>(n);
     const double r1 = fma(-nd, 0x1.921fb54400000p+0, a);
     *quadrant = n & 3;
@@ -219,7 +230,7 @@ RG_HDI float game_quat_quant_component(float c) {
     const float max_f = static_cast<float>(kMax);
     float v = ((c * 1.41421354f) * 0.5f + 0.5f) * max_f;
     v = (v + v) + 0.5f;
-    int k = static_cast<int>(rintf(v));
+    int k = x86_f2i(rintf(v));
     k = k < 0 ? (k - 1) / 2 : k / 2;
     k = k < 0 ? 0 : (k < kMax ? k : kMax);
     const float r = static_cast<float>(k) / max_f - 0.5f;
@@ -255,7 +266,7 @@ RG_HDI Q4 game_quantize_basis(V3& fwd, V3& right, V3& up) {
 // by a tenth of a step away from zero) applied at every tick start (reference raycast_wheels_and_contact_prep.hpp:3851-3871).
 RG_HDI float quant_trunc_offset(float x, float scale) {
     const float inv_scale = 1.0f / scale;
-    const float k = static_cast<float>(static_cast<int32_t>(x * scale));
+    const float k = static_cast<float>(x86_f2i(x * scale));
     const float rounded = k * inv_scale;
     const float offset_mag = 0.1f * inv_scale;
     const float sgn = rounded == 0.0f ? 0.0f : (rounded > 0.0f ? 1.0f : -1.0f);

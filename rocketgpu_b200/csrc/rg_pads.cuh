@@ -310,7 +310,7 @@ RG_NOINL void pads_tail(CarState* cars, int car_base, int max_cars, const CarCon
             PadState& pad = pads[p];
             if (pad.is_active && pad.cur_locked_car_id == 0 && pad_eligible(c, tc)) {
                 pad.cur_locked_car_id = static_cast<uint32_t>(car_base + i + 1);
-                const int whole = static_cast<int>(c.boost);
+                const int whole = x86_f2i(c.boost);
                 c.rlbotv5_boost_hold = static_cast<uint8_t>(
                     (254 < whole + (static_cast<float>(whole) < c.boost ? 1 : 0)
                          ? 254

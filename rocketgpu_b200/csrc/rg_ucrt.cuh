@@ -70,7 +70,7 @@ RG_HDI float ucrt_atan2f(float yf, float xf) {
     const double ratio = u / v;
     double res;
     if (ratio > 0x1p-4) {
-        const int i = static_cast<int>(fma(256.0, ratio, 0.5));
+        const int i = x86_d2i(fma(256.0, ratio, 0.5));
         const double id = static_cast<double>(i);
         const double r = fma(u, 256.0, -(id * v)) / fma(u, id, v * 256.0);
         res = fma(-((r * r) * r), 0x1.5555555550877p-2, r + RG_UCRT_TAB(kAtanTab)[i - 16]);
@@ -91,7 +91,7 @@ RG_HDI float ucrt_atan2f(float yf, float xf) {
 RG_HDI float ucrt_powf_exp(double t, uint32_t sign, bool fused) {
     if (t > 0x1.62e43p6) return u2f(0x7f800000u | sign);
     if (!(t > -0x1.9d1dap6)) return u2f(sign);
-    const int n = static_cast<int>(rint(t * 0x1.71547652b82fep+6));
+    const int n = x86_d2i(rint(t * 0x1.71547652b82fep+6));
     const double tab = RG_UCRT_TAB(kPowExp2)[n & 63];
     double res;
     if (fused) {

@@ -124,7 +124,8 @@ def test_pybind_module_mirrors_the_reference_binding(arena_mesh):
                  "upload_boost_pad_states", "upload_controls", "download_car_states", "download_ball_states",
                  "download_env_states", "download_boost_pad_states", "upload_state_array", "download_state_array",
                  "apply_env_commands", "apply_env_commands_device", "step", "step_with_device_controls",
-                 "step_with_device_commands", "reset_to_kickoff", "synchronize"):
+                 "step_with_device_commands", "reset_to_kickoff", "synchronize", "internal_state_layout",
+                 "download_internal_state", "upload_internal_state"):
         assert hasattr(m.BatchSim, name), name
     cfg = m.SimConfig()
     assert cfg.kickoff_settled == 0 and cfg.max_cars_per_env == 6

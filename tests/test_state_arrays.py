@@ -78,6 +78,52 @@ def test_state_arrays_by_name_and_device_arrays(oracle_available, arena_mesh):
         assert parity.equal(orc.balls(), gpu.download_ball_states()), preserve
 
 
+def test_internal_state_snapshot_restores_a_batch(arena_mesh):
+    """Public arrays (PreserveInternal) plus the internal state blob are a whole snapshot: restoring one into the
+    batch and replaying the same controls repeats the same ticks byte for byte (reference download/upload_internal_
+    state, python/rocketgpu_bindings.cpp:1002-1060)."""
+    import torch
+    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
+    v, i = arena_mesh
+    n, mc = 48, 4
+    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=mc), v, i)
+    counts = np.array([2, 4, 3] * (n // 3), np.int32)
+    gpu.set_env_car_count(counts)
+    gpu.set_teams(np.tile(np.array([0, 1, 0, 1], np.uint8), n))
+    gpu.reset_to_kickoff(9)
+    crng = np.random.default_rng(9)
+    for _ in range(60):
+        ctrl = scenarios.chase_ball_controls(gpu.download_car_states(), gpu.download_ball_states(), mc, crng)
+        gpu.step_with_device_controls(torch.from_numpy(ctrl).cuda().data_ptr(), 1, 0)
+    gpu.synchronize()
+    layout = gpu.internal_state_layout()
+    assert [name for name, _ in layout] == ["wheel_runtime", "ball_world", "broadphase", "car_world", "ball_car",
+                                            "car_pairs", "car_stages"]
+    public = {name: getattr(gpu, f"download_{name}")() for name in ("car_states", "ball_states", "env_states",
+                                                                    "boost_pad_states")}
+    blob = gpu.download_internal_state()
+    replay = [scenarios.chase_ball_controls(public["car_states"], public["ball_states"], mc, crng) for _ in range(8)]
+
+    def run():
+        outs = []
+        for k in range(40):
+            gpu.step_with_device_controls(torch.from_numpy(replay[k % 8]).cuda().data_ptr(), 1, 0)
+        gpu.synchronize()
+        for name in public:
+            outs.append(getattr(gpu, f"download_{name}")())
+        outs.append(gpu.download_internal_state())
+        return outs
+    first = run()
+    for name, arr in public.items():
+        gpu.upload_state_array(name, arr.ctypes.data, len(arr), True)
+    gpu.upload_internal_state(blob)
+    assert np.array_equal(gpu.download_internal_state(), blob)
+    second = run()
+    for a, b in zip(first, second):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(first[0], public["car_states"])
+
+
 def test_pybind_module_steps_like_the_oracle(oracle_available, arena_mesh):
     """The pybind11 module with the reference binding's names: a mixed batch driven through it matches the oracle."""
     import importlib
