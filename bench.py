@@ -202,9 +202,9 @@ class MixedWorkload:
 
 
 def _presets():
-    """The six hitbox presets as the oracle exports them (byte-identical CarConfig rows)."""
-    from tests import oracle_ref
-    return [oracle_ref.car_preset(k) for k in range(6)]
+    """The six hitbox presets (CarConfig rows) from the library."""
+    from rocketgpu_b200.batch_sim import car_preset
+    return [car_preset(k) for k in range(6)]
 
 
 def arena_hashes(rows: np.ndarray, per_arena: int) -> np.ndarray:

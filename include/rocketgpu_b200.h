@@ -210,6 +210,10 @@ RG_API void rg_default_env_state(rg_env_state* out);
 /* CarState{} and CarConfig{} (the Octane preset) — reference rocketgpu.h:135-175, 190-502. */
 RG_API void rg_default_car_state(rg_car_state* out);
 RG_API void rg_default_car_config(rg_car_config* out);
+/* The hitbox presets: 0 Octane (= rg_default_car_config), 1 Dominus, 2 Plank, 3 Breakout, 4 Hybrid, 5 Merc
+ * (reference OctaneConfig .. MercConfig, src/rocketgpu.cpp:417-490; Python binding OctaneConfig() ..). out_of_range
+ * for any other index. */
+RG_API int rg_car_preset(int32_t preset, rg_car_config* out);
 
 /* BatchSim(config, layout) — reference rocketgpu.h:990-992, src/rocketgpu.cpp:1019-1250. Validates the config
  * (env_count > 0, 0 <= max_cars_per_env <= 8) and layout (finite, within 11,500 uu), builds the mesh BVH on the

@@ -28,7 +28,7 @@ EXPORTS = [
     "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
     "rg_batch_set_launch_config", "rg_batch_get_launch_config", "rg_batch_upload_state_array",
     "rg_batch_download_state_array", "rg_batch_internal_state_layout", "rg_batch_download_internal_state",
-    "rg_batch_upload_internal_state",
+    "rg_batch_upload_internal_state", "rg_car_preset",
 ]
 
 
@@ -116,6 +116,7 @@ def lib():
         L.rg_batch_step_static_scratch.argtypes = [vp, vp, vp, i32, i32, i32, vp]
         L.rg_default_car_state.argtypes = [vp]
         L.rg_default_car_config.argtypes = [vp]
+        L.rg_car_preset.argtypes = [i32, vp]
         L.rg_batch_pad_capacity.argtypes = [vp]
         L.rg_batch_pad_capacity.restype = i64
         L.rg_batch_step_with_device_controls.argtypes = [vp, vp, i32, i32, vp]

@@ -40,6 +40,18 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+PRESETS = ("octane", "dominus", "plank", "breakout", "hybrid", "merc")
+
+
+def car_preset(preset) -> np.ndarray:
+    """One hitbox preset as a raw CarConfig row (120 bytes): index 0-5 or name (reference OctaneConfig() ..
+    MercConfig(), src/rocketgpu.cpp:417-490)."""
+    k = PRESETS.index(preset.lower()) if isinstance(preset, str) else int(preset)
+    out = np.zeros(120, np.uint8)
+    _check(abi.lib().rg_car_preset(k, _ptr(out)))
+    return out
+
+
 class SimConfig:
     """The reference SimConfig / MutatorConfig fields this path takes (defaults as the reference's)."""
 

@@ -870,6 +870,76 @@ RG_API void rg_default_car_config(rg_car_config* o) {
     o->spawn_z = 36.02f;
 }
 
+// The game's hitbox presets (reference OctaneConfig .. MercConfig, src/rocketgpu.cpp:417-490): hitbox (published size
+// + 2.5 uu per axis), offsets, wheel radii and suspension rest lengths, steering curves, spawn height, body id. The
+// numbers are the game's car data, the same in every implementation.
+namespace {
+struct PresetData {
+    float hitbox[3], hitbox_offset[3];
+    float front_radius, front_rest, front_offset[3];
+    float back_radius, back_rest, back_offset[3];
+    float steer[6], powerslide[2];
+    bool own_steer;
+    float spawn_z;
+    uint16_t body;
+};
+constexpr PresetData kPresets[] = {
+    // Dominus
+    {{127.92678f, 83.27995f, 31.3f}, {9.0f, 0.0f, 15.75f}, 12.00f, 33.95f, {50.30f, 31.10f, 15.75f}, 13.50f, 33.85f,
+     {-34.75f, 33.00f, 15.75f},
+     {29.923809051513672f, 18.018766403198242f, 10.329229354858398f, 6.019903182983398f, 4.85035514831543f,
+      1.9751166105270386f},
+     {22.08690071105957f, 7.173928260803223f}, true, 36.01f, 132},
+    // Plank
+    {{128.81978f, 84.670364f, 29.394402f}, {9.008572f, 0.0f, 12.0942f}, 12.50f, 31.9242f, {49.97f, 27.799904f, 12.0942f},
+     17.00f, 27.9242f, {-35.43f, 20.280005f, 12.0942f},
+     {30.342710494995117f, 18.1981258392334f, 10.394840240478516f, 6.043498516082764f, 4.865903377532959f,
+      1.9777874946594238f},
+     {22.341325759887695f, 7.206938743591309f}, true, 38.84f, 150},
+    // Breakout
+    {{131.49236f, 80.521f, 30.3f}, {12.5f, 0.0f, 11.75f}, 13.50f, 29.7f, {51.50f, 26.67f, 11.75f}, 15.00f, 29.66f,
+     {-35.75f, 35.00f, 11.75f},
+     {30.55976104736328f, 18.289745330810547f, 10.42794418334961f, 6.055309772491455f, 4.873669147491455f,
+      1.9791138172149658f},
+     {22.472003936767578f, 7.2235002517700195f}, true, 36.00f, 64},
+    // Hybrid
+    {{127.01919f, 82.18787f, 34.159073f}, {13.87566f, 0.0f, 20.754988f}, 12.50f, 38.75499f, {51.25f, 25.90f, 20.754988f},
+     15.00f, 37.054989f, {-34.00f, 29.50f, 20.754988f},
+     {30.580455780029297f, 18.29843521118164f, 10.431071281433105f, 6.056422233581543f, 4.874399185180664f,
+      1.9792383909225464f},
+     {22.484424591064453f, 7.225060939788818f}, true, 37.53f, 56},
+    // Merc (keeps the default steering curves)
+    {{120.72023f, 76.71031f, 41.659073f}, {11.37566f, 0.0f, 21.504988f}, 15.00f, 39.50499f, {51.25f, 25.90f, 21.504988f},
+     15.00f, 39.104988f, {-33.75f, 29.50f, 21.504988f}, {}, {}, false, 35.05f, 219},
+};
+}  // namespace
+
+RG_API int rg_car_preset(int32_t preset, rg_car_config* out) {
+    return guard([&] {
+        if (!out) throw std::invalid_argument("null argument");
+        if (preset < 0 || preset > 5) throw std::out_of_range("preset must be 0..5 (Octane .. Merc)");
+        rg_default_car_config(out);
+        if (preset == 0) return;
+        const PresetData& d = kPresets[preset - 1];
+        out->hitbox_published = {d.hitbox[0], d.hitbox[1], d.hitbox[2]};
+        out->hitbox_size = {d.hitbox[0] + 2.5f, d.hitbox[1] + 2.5f, d.hitbox[2] + 2.5f};
+        out->hitbox_offset = {d.hitbox_offset[0], d.hitbox_offset[1], d.hitbox_offset[2]};
+        out->front_wheels_offset = {d.front_offset[0], d.front_offset[1], d.front_offset[2]};
+        out->back_wheels_offset = {d.back_offset[0], d.back_offset[1], d.back_offset[2]};
+        out->front_wheel_radius = d.front_radius;
+        out->back_wheel_radius = d.back_radius;
+        out->front_suspension_rest = d.front_rest;
+        out->back_suspension_rest = d.back_rest;
+        out->three_wheels = 0;
+        if (d.own_steer) {
+            std::memcpy(out->steer_angle_curve_deg, d.steer, sizeof(d.steer));
+            std::memcpy(out->powerslide_steer_angle_curve_deg, d.powerslide, sizeof(d.powerslide));
+        }
+        out->spawn_z = d.spawn_z;
+        out->body = d.body;
+    });
+}
+
 RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layout, int device, rg_batch** out) {
     return guard([&] {
         if (!cfg || !layout || !out) throw std::invalid_argument("null argument");

@@ -38,6 +38,17 @@ def test_defaults_match_reference_structs(oracle_available):
     assert (my_cfg[keep] == cfg[keep]).all(), np.nonzero(my_cfg != cfg)[0]
 
 
+def test_car_presets_match_reference(oracle_available):
+    from rocketgpu_b200.batch_sim import car_preset
+    from tests import oracle_ref
+    keep = np.arange(120) != 81  # CarConfig's padding byte
+    for k in range(6):
+        assert (car_preset(k)[keep] == oracle_ref.car_preset(k)[keep]).all(), k
+    assert (car_preset("merc") == car_preset(5)).all()
+    with pytest.raises(IndexError):
+        car_preset(6)
+
+
 def test_ucrt_math_matches_reference(oracle_available):
     from tests import oracle_ref
     L = oracle_ref.lib()

@@ -107,8 +107,11 @@ def test_step_with_device_commands(oracle_available, arena_mesh):
         cmds[rng.integers(0, k, len(sel)), sel] = _random_commands(rng, len(sel))
         cmds[:, :, 6:8] = 0
         orc.step_with_commands(ctrl, 0, cmds.reshape(-1, 16), n, k)
-        gpu.step_with_device_commands(torch.from_numpy(ctrl).cuda().data_ptr(), 0,
-                                      torch.from_numpy(cmds.reshape(-1, 16).copy()).cuda().data_ptr(), n, k)
+        # both device buffers stay referenced until the step has run (a temporary's memory could be handed to the
+        # next allocation before the stream reads it)
+        dev_ctrl = torch.from_numpy(ctrl).cuda()
+        dev_cmds = torch.from_numpy(cmds.reshape(-1, 16).copy()).cuda()
+        gpu.step_with_device_commands(dev_ctrl.data_ptr(), 0, dev_cmds.data_ptr(), n, k)
         gpu.synchronize()
         d = _compare(orc, gpu, counts)
         assert d is None, f"step {step}: {d}"
