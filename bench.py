@@ -39,6 +39,7 @@ threads, on the same workload, settle, warm-up and timed steps).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import ctypes
 import json
 import os
@@ -54,6 +55,7 @@ sys.path.insert(0, ROOT)
 
 ENVS = 16384
 TICKS_PER_STEP = 8
+KERNELS_PER_TICK = 7  # arena begin, car tick start, wheel rays, vehicle updates, arena finish, car post-tick, arena tail
 SETTLE_STEPS = 40
 NO_TOUCH_TICKS = 300
 MAX_CARS = 6
@@ -393,12 +395,14 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
+        torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps' launches by this range
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
             step(sim_a, cmds_a, timed_dev[k].data_ptr() if mixed else None)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     phase_ms = (ctypes.c_float * 6)()
@@ -460,7 +464,7 @@ def run_ours(args, world, rank, local):
                                 "max": float(np.max(step_ms)), "e2e_p50": float(np.percentile(e2e_ms, 50)),
                                 "e2e_p99": float(np.percentile(e2e_ms, 99))},
         "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps * (TICKS_PER_STEP * 6 + 1) if mixed else args.steps,
+        "gpu_launches": args.steps * (TICKS_PER_STEP * KERNELS_PER_TICK + 1) if mixed else args.steps,
         "clocks": clocks.summary(),
     }
     if mixed:
@@ -481,6 +485,8 @@ def run_ours(args, world, rank, local):
             "note": "dominant kernel by device time; the tick is bound by latency and FP32 issue of serial per-arena "
                     "work, not by HBM; frac is the HBM fraction of its algorithmic state bytes"}
         line["kernel_ms_per_step"] = {name: ms * TICKS_PER_STEP for name, ms in per_launch_ms.items()}
+        # the same digest as the reference CUDA arm's (--impl reference --ref-backend cuda) after the same ticks
+        line["final_state_sha"] = hashlib.sha256(final_a[0].tobytes() + final_a[1].tobytes()).hexdigest()[:16]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         timing, record = cpu_leg(args.workload, args.warmup, args.steps, parity=True)
         line["cpu_baseline"] = timing
@@ -643,12 +649,72 @@ def run_reference(args, world, rank):
     return line
 
 
+def run_reference_cuda(args, world, rank):
+    """The reference's own CUDA build of the path (oracle/_ref/librg_oracle_cuda.so: src/rocketgpu_cuda.cu and the host
+    sources compiled here for sm_100 with ROCKETGPU_USE_CUDA) on the same workload, stepped through its BatchSim with
+    device-resident controls and commands: the plain GPU bar. Each step is timed host-side with a device
+    synchronisation on both sides (the reference launches on its own streams); the episode clock's commands are made
+    between steps, outside the timed region, as in the CPU leg."""
+    import torch
+    if rank != 0:
+        return None
+    from rocketgpu_b200 import arena
+    from tests import oracle_ref, scenarios
+    path = os.path.join(ROOT, "oracle", "_ref", "librg_oracle_cuda.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/librg_oracle_cuda.so not built (make -C oracle cuda)"}
+    oracle_ref.LIB_PATH = path
+    oracle_ref._lib = None
+    v, i = arena.generate()
+    w = MixedWorkload(0)
+    sim = oracle_ref.OracleSim(ENVS, MAX_CARS, v, i, kickoff_settled=False)
+    sim.set_env_car_count(w.counts)
+    sim.set_teams(w.teams)
+    sim.set_car_configs(w.car_configs(_presets()))
+    sim.reset_to_kickoff(w.reset_seed)
+    clock = scenarios.EpisodeClock(sim.envs(), sim.cars(), MAX_CARS, NO_TOUCH_TICKS, w.stagger_seed)
+    cmds = np.zeros((TICKS_PER_STEP * ENVS, CMD_BYTES), np.uint8)
+    ctrl_dev = torch.empty(TICKS_PER_STEP * ENVS * MAX_CARS * CTRL_BYTES, dtype=torch.uint8, device="cuda")
+    cmd_dev = torch.empty(TICKS_PER_STEP * ENVS * CMD_BYTES, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    gen = w.controls()
+    step_s = []
+    for k in range(SETTLE_STEPS + args.warmup + args.steps):
+        ctrl_dev.copy_(torch.from_numpy(next(gen).reshape(-1)))
+        cmd_dev.copy_(torch.from_numpy(cmds.reshape(-1)))
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.step_with_device_commands(ctrl_dev.data_ptr(), ENVS * MAX_CARS, cmd_dev.data_ptr(), ENVS, TICKS_PER_STEP)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if k >= SETTLE_STEPS + args.warmup:
+            step_s.append(dt)
+        cmds[:ENVS] = clock.commands(sim.envs(), sim.cars(), w.counts)
+    final = (_active_car_rows(sim.cars(), w.counts), sim.balls())
+    sim.close()
+    value = ENVS * TICKS_PER_STEP * len(step_s) / sum(step_s)
+    ms = sorted(1e3 * s for s in step_s)
+    return {
+        "impl": "reference", "backend": "cuda", "metric": METRIC, "value": value, "unit": "arena-ticks/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(step_s) / len(step_s),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded arenas, bodies, controls and episode resets)",
+        "config": {"workload": WORKLOADS["mixed"], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
+                   "settle_steps": SETTLE_STEPS, "l2": "256 MiB flush before every timed step"},
+        "latency_ms_per_step": {"p50": ms[len(ms) // 2], "p99": ms[min(len(ms) - 1, int(0.99 * len(ms)))]},
+        "final_state_sha": hashlib.sha256(final[0].tobytes() + final[1].tobytes()).hexdigest()[:16],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-backend", default="cpu", choices=["cpu", "cuda"],
+                    help="reference arm: its CPU BatchSim (default) or its own CUDA build (the plain GPU bar)")
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--arenas", type=int, default=ENVS, help="arenas per GPU (smaller cases for profiling)")
@@ -664,7 +730,7 @@ def main():
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
-        line = run_reference(args, world, rank)
+        line = run_reference_cuda(args, world, rank) if args.ref_backend == "cuda" else run_reference(args, world, rank)
     else:
         world, rank, local = dist_setup(args.gpus)
         line = run_serve(args, world, rank, local) if args.workload == "serve" else run_ours(args, world, rank, local)

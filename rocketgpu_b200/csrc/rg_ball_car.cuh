@@ -413,11 +413,10 @@ RG_HDI void ball_car_point_rows(BallCarRows& rows, const BallState& b, const Car
     fr.normal_row = vi;
 }
 
-// The car's contact with the ball this tick: fresh geometry merged into the retained manifold, rows per point
-// (reference AppendBallCarContactRowsRetained).
-RG_NOINL void ball_car_contacts(BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
-                              const TickConfig& tc, int car, V3 ball_ext_uu, V3 ball_lin_bt, float dt,
-                              BallCarRows& rows) {
+// The geometry half of a car's ball contact: this tick's fresh contact merged into the retained manifold. It reads
+// only the two bodies' poses.
+RG_HDI void ball_car_manifold_update(BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
+                                     const TickConfig& tc) {
     const float thr = ball_car_threshold_bt(cfg, tc.ball_radius);
     BallCarGeom g;
     const bool fresh = ball_car_geometry(b, c, cfg, tc.ball_radius, thr, g);
@@ -455,7 +454,22 @@ RG_NOINL void ball_car_contacts(BallCarScratch& m, const BallState& b, const Car
             for (int i = 0; i < fc; ++i) ball_car_add(m, fp[i], thr);
         }
     }
+}
+
+// The rows half: the rows of every retained point, from the bodies' velocities at the world step.
+RG_HDI void ball_car_manifold_rows(const BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
+                                   const TickConfig& tc, int car, V3 ball_ext_uu, V3 ball_lin_bt, float dt,
+                                   BallCarRows& rows) {
     for (int i = 0; i < m.count; ++i) ball_car_point_rows(rows, b, c, cfg, tc, car, m.pts[i], ball_ext_uu, ball_lin_bt, dt);
+}
+
+// The car's contact with the ball this tick: fresh geometry merged into the retained manifold, rows per point
+// (reference AppendBallCarContactRowsRetained).
+RG_NOINL void ball_car_contacts(BallCarScratch& m, const BallState& b, const CarState& c, const CarConfig& cfg,
+                              const TickConfig& tc, int car, V3 ball_ext_uu, V3 ball_lin_bt, float dt,
+                              BallCarRows& rows) {
+    ball_car_manifold_update(m, b, c, cfg, tc);
+    ball_car_manifold_rows(m, b, c, cfg, tc, car, ball_ext_uu, ball_lin_bt, dt, rows);
 }
 
 // ---- the ball hit ------------------------------------------------------------------------------------------------

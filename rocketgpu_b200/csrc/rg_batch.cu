@@ -404,6 +404,20 @@ __global__ void __launch_bounds__(256) car_pre_kernel(CarTickArgs a, int t) {
 // Tick part 3, one thread per active car: the vehicle update (four suspension rays against the arena mesh and the
 // ball, tyres, drive, air control) and the car's staged world-step parts, for cars whose wheels can land on no other
 // car and under whose car no other wheel can land (rg::arena_free_cars); the others are left to part 4.
+// Tick part 3a, one thread per wheel of an active car: the wheel's suspension ray against the arena mesh, cast ahead of
+// the car's vehicle update (it reads only the car's pose and config, final once the car's tick start has run).
+__global__ void __launch_bounds__(256) car_rays_kernel(CarTickArgs a, int t) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g >> 2, wheel = g & 3;
+    if (k >= a.active_car_count) return;
+    const int idx = a.active_cars[k];
+    const int e = idx / a.max_cars;
+    if (arena_idle(a, e)) return;
+    const rg::CarState& car = a.cars[idx];
+    if (car.is_demoed) return;  // a demolished car's vehicle update casts no rays
+    rg::wheel_mesh_ray_ahead(car, a.car_cfgs[idx], arena_mesh(a.base, e), wheel, a.stages[idx].wheel_mesh[wheel]);
+}
+
 __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.active_car_count) return;
@@ -415,6 +429,9 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
     const bool free =
         (rg::arena_free_cars(a.cars + base, a.car_cfgs + base, a.broadphase[e], count) >> (idx - base)) & 1u;
     a.stages[idx].in_car_thread = free ? 1u : 0u;
+    // every car's ball contact geometry, before its vehicle update (it reads poses only)
+    rg::car_ball_stage(a.base.balls[e], a.snaps[e].ball_vel_bt, a.cars[idx], a.car_cfgs[idx], a.base.tc,
+                       a.records[idx].vel_bt, a.records[idx].ang_vel, a.ball_car[idx], a.stages[idx]);
     if (!free) return;  // the arena thread updates this car in the game's car order
     const rg::CarControls& ctrl =
         a.controls[control_row(a, e, t) * static_cast<size_t>(a.control_stride) + static_cast<size_t>(idx)];
@@ -424,7 +441,8 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
                                                               count);
     const rg::MeshDevice& mesh = arena_mesh(a.base, e);
     rg::vehicle_update(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], a.base.balls[e], mesh,
-                       rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes);
+                       rg::WheelOthers{nullptr, nullptr, 0, -1, excluded}, a.records[idx].pushes,
+                       a.stages[idx].wheel_mesh);
     // the car's own part of the world step, while this thread has the car (rg::CarStage)
     rg::car_stage_compute(a.cars[idx], a.car_cfgs[idx], a.wheels[idx], a.car_world[idx], a.base.tc, mesh, idx - base,
                           a.records[idx].vel_bt, a.records[idx].ang_vel, a.stages[idx]);
@@ -535,6 +553,7 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
     const int blocks = (b->env_count + threads - 1) / threads;
     const int ct = b->car_threads;
     const int car_blocks = (b->active_car_count + ct - 1) / ct;
+    const int wheel_blocks = (4 * b->active_car_count + ct - 1) / ct;
     auto mark = [&] {
         if (!b->timing) return;
         if (b->events_used == b->events.size()) {
@@ -550,6 +569,8 @@ void launch_car_tick(rg_batch* b, const rg::CarControls* controls, int stride, i
         mark();
         if (car_blocks) car_pre_kernel<<<car_blocks, ct, 0, s>>>(a, t);
         mark();
+        // phase 2 (timing) is the wheel rays and the vehicle updates
+        if (car_blocks) car_rays_kernel<<<wheel_blocks, ct, 0, s>>>(a, t);
         if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s>>>(a, t);
         mark();
         arena_finish_kernel<<<blocks, threads, 0, s>>>(a, t);

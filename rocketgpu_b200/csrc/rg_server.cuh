@@ -129,6 +129,7 @@ void server_launch_round(rg_server* s) {
     const int car_blocks = (b->active_car_count + ct - 1) / ct;
     arena_begin_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
     if (car_blocks) car_pre_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
+    if (car_blocks) car_rays_kernel<<<(4 * b->active_car_count + ct - 1) / ct, ct, 0, s->stream>>>(a, 0);
     if (car_blocks) car_vehicle_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0);
     arena_finish_kernel<<<blocks, threads, 0, s->stream>>>(a, 0);
     if (car_blocks) car_post_kernel<<<car_blocks, ct, 0, s->stream>>>(a, 0, 0);

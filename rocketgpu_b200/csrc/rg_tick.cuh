@@ -1043,6 +1043,9 @@ struct CarStage {
     BpProxy proxy;       // the car's broadphase proxy (valid = 0 for a car demolished at the step's start)
     PadContacts pads;    // the car's pad contacts after its post-tick (pad_contacts_stage)
     uint32_t in_car_thread;  // this tick's vehicle update and stage ran in the car's own thread (arena_free_cars)
+    RayHit wheel_mesh[4];    // the wheels' arena-mesh rays, cast ahead of the vehicle update (wheel_mesh_ray_ahead)
+    BallCarScratch ball_manifold;  // the car/ball manifold after this tick's geometry (car_ball_stage)
+    uint32_t ball_staged;          // ball_manifold holds this tick's update
 };
 
 // A car's broadphase proxy: its box now and at the pose this tick's tick-start velocities predict (reference
@@ -1054,6 +1057,30 @@ RG_HDI void car_body_proxy(BpProxy& p, const CarState& car, const CarConfig& cfg
     game_integrate_orientation(px, py, pz, unused, ang_vel, dt);
     car_proxy(p, car.pos_bt, ax, ay, az, px, py, pz, vel_bt, cfg.hitbox_offset * (1.0f / 50.0f), car_box_half_bt(cfg),
               dt);
+}
+
+// The car's ball contact geometry ahead of the world step (one thread per car). The manifold update reads only the
+// two bodies' poses, and neither body moves between the tick start and the world step's car-ball stage (vehicle
+// updates, wheel pushes, bumps and demolitions change velocities and flags only). Staged when the car's box or swept
+// proxy meets the ball's, a superset of the world step's test; the world step takes it when its own test passes.
+RG_HDI void car_ball_stage(const BallState& b, V3 ball_start_vel_bt, const CarState& car, const CarConfig& cfg,
+                           const TickConfig& c, V3 start_vel_bt, V3 start_ang_vel, const BallCarScratch& m_in,
+                           CarStage& st) {
+    st.ball_staged = 0u;
+    if (car.is_demoed || car.just_respawned) return;  // the world step's tests fail for both
+    bool meet = ball_car_box_overlaps(b, car, cfg, c, true);
+    if (!meet) {
+        BpProxy pb, pc;
+        ball_proxy(pb, b.pos_bt, ball_start_vel_bt, c.ball_radius, c.tick_dt);
+        car_body_proxy(pc, car, cfg, start_vel_bt, start_ang_vel, c.tick_dt);
+        meet = pc.valid != 0 && !(pc.child_min.x > pb.child_max.x || pc.child_max.x < pb.child_min.x ||
+                                  pc.child_min.y > pb.child_max.y || pc.child_max.y < pb.child_min.y ||
+                                  pc.child_min.z > pb.child_max.z || pc.child_max.z < pb.child_min.z);
+    }
+    if (!meet) return;
+    st.ball_manifold = m_in;
+    ball_car_manifold_update(st.ball_manifold, b, car, cfg, c);
+    st.ball_staged = 1u;
 }
 
 RG_HDI void car_stage_compute(CarState& car, const CarConfig& cfg, WheelRuntime& w, const CarWorldScratch& ws_in,
@@ -1212,7 +1239,12 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
             bcs[i].count = 0;
             continue;
         }
-        ball_car_contacts(bcs[i], b, car, A.cfgs[i], c, i, ext_delta, solver_vel_bt, sub_dt, bc);
+        if (stages && stages[i].ball_staged) {
+            bcs[i] = stages[i].ball_manifold;
+            ball_car_manifold_rows(bcs[i], b, car, A.cfgs[i], c, i, ext_delta, solver_vel_bt, sub_dt, bc);
+        } else {
+            ball_car_contacts(bcs[i], b, car, A.cfgs[i], c, i, ext_delta, solver_vel_bt, sub_dt, bc);
+        }
         if (!pre[i].is_demoed && !car.just_respawned)
             commit_ball_hit_from_manifold(b, car, bcs[i], static_cast<uint32_t>(A.car_base + i + 1), env_tick,
                                           hit_car_pos[i], hit_car_rot[i], hit_ball_pos, snap.car_start_vel[i],
@@ -1455,7 +1487,7 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
         left |= 1u << i;
         const uint32_t excluded = A.cars[i].is_demoed ? 0u : wheel_ray_excluded_bodies(A.cars[i], A.cfgs[i], &bp, i, count);
         vehicle_update(A.cars[i], A.controls[i], A.cfgs[i], c, A.wheels[i], b, mesh,
-                       WheelOthers{A.cars, A.cfgs, count, i, excluded}, recs[i].pushes);
+                       WheelOthers{A.cars, A.cfgs, count, i, excluded}, recs[i].pushes, stages[i].wheel_mesh);
     }
     for (int i = 0; i < count; ++i)
         if ((left >> i) & 1u)

@@ -485,15 +485,16 @@ RG_HDI bool wheel_ray_vs_car_box(V3 src, V3 dir, float max_len, float max_len_bt
 
 // One suspension ray against the arena mesh, the arena's other cars and the ball (reference RayCastWheelAgainstArena,
 // :641-845, with CastWheelRayAgainstCars :329-421, on a meshes-only arena).
-RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& ball, const TickConfig& tc,
-                           const MeshDevice& mesh, float min_hit_dist_sq_bt, const WheelOthers& oth) {
+// The arena-mesh part of a wheel's suspension ray. It reads only the wheel's ray (the car's pose and config), which
+// nothing changes between the car's tick start and its vehicle update, so it may run ahead of the update.
+RG_HDI void wheel_mesh_ray(const WheelStep& w, const MeshDevice& mesh, float min_hit_dist_sq_bt, RayHit& hit) {
     const float real_ray_length =
         w.suspension_rest_length + w.max_suspension_travel + w.wheel_radius - kWheelSuspensionSubtraction;
     const float real_ray_length_bt = (w.suspension_rest_length * kUuToBt + w.wheel_radius * kUuToBt) +
                                      (w.max_suspension_travel - kWheelSuspensionSubtraction) * kUuToBt;
-    RayHit hit;
     hit.hit = 0;
     hit.t = 0.0f;
+    hit.point_bt = hit.normal = V3{0.0f, 0.0f, 0.0f};
     hit.kind = kRayHitUnknown;
     hit.mesh_index = -1;
     {
@@ -517,6 +518,23 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
             hit.kind = kRayHitArenaMesh;
             hit.mesh_index = 0;
         }
+    }
+}
+
+// A wheel's suspension ray against the arena mesh (or its result `mesh_hit`, cast ahead by wheel_mesh_ray), the
+// other cars' boxes and the ball; the closest hit becomes the wheel's contact.
+RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& ball, const TickConfig& tc,
+                           const MeshDevice& mesh, float min_hit_dist_sq_bt, const WheelOthers& oth,
+                           const RayHit* mesh_hit = nullptr) {
+    const float real_ray_length =
+        w.suspension_rest_length + w.max_suspension_travel + w.wheel_radius - kWheelSuspensionSubtraction;
+    const float real_ray_length_bt = (w.suspension_rest_length * kUuToBt + w.wheel_radius * kUuToBt) +
+                                     (w.max_suspension_travel - kWheelSuspensionSubtraction) * kUuToBt;
+    RayHit hit;
+    if (mesh_hit) {
+        hit = *mesh_hit;
+    } else {
+        wheel_mesh_ray(w, mesh, min_hit_dist_sq_bt, hit);
     }
     bool hit_world = hit.hit != 0;
     int32_t ground_car_idx = -1;
@@ -1025,9 +1043,10 @@ RG_HDI void apply_wheel_ball_pushes(BallState& ball, const WheelBallPushes& p, c
     }
 }
 
+// `mesh_hits`: the four wheels' arena-mesh rays cast ahead (wheel_mesh_ray_ahead), or null to cast them here.
 RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg, const TickConfig& tc,
                            WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, const WheelOthers& oth,
-                           WheelBallPushes& pushes) {
+                           WheelBallPushes& pushes, const RayHit* mesh_hits = nullptr) {
     pushes.count = 0;
     const float dt = tc.tick_dt;
     c.demo_no_contact_response = c.is_demoed ? 1 : 0;
@@ -1077,7 +1096,7 @@ RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cf
             init_wheel(w, c, cfg, i, f, i < 2 ? front_bone : back_bone);
             w.suspension_force_scale = w.is_front_wheel ? front_scale : back_scale;
             w.extra_pushback = wr.extra_pushback[i];
-            wheel_ray_cast(c, w, ball, tc, mesh, min_hit_dist_sq, oth);
+            wheel_ray_cast(c, w, ball, tc, mesh, min_hit_dist_sq, oth, mesh_hits ? mesh_hits + i : nullptr);
             if (w.is_in_contact) w.extra_pushback = 0.0f;
             if (w.is_in_contact_with_world) world_wheel_pushback(c, tc, w, f);
             if (w.is_in_contact && !w.is_in_contact_with_world && w.ground_kind == kRayHitCar && oth.cars &&
@@ -1296,6 +1315,18 @@ struct PreContactCar {
     V3 vel, vel_bt, ang_vel;
     uint8_t is_demoed;
 };
+// Wheel `i`'s arena-mesh ray as the car's vehicle update casts it (the same wheel set-up from the car's pose and
+// config), for running the rays of every car ahead of the updates, one thread per wheel.
+RG_HDI void wheel_mesh_ray_ahead(const CarState& c, const CarConfig& cfg, const MeshDevice& mesh, int i, RayHit& hit) {
+    CarFrame f;
+    car_basis(c, f.fwd, f.right, f.up);
+    float front_bone, back_bone;
+    wheel_bone_z(cfg, front_bone, back_bone);
+    WheelStep w;
+    init_wheel(w, c, cfg, i, f, i < 2 ? front_bone : back_bone);
+    wheel_mesh_ray(w, mesh, min_wheel_hit_dist_sq_bt(cfg), hit);
+}
+
 RG_HDI void car_world_prestep(CarState& c, const CarConfig& cfg, const WheelRuntime& wr, const TickConfig& tc,
                               float sub_dt, PreContactCar& pre) {
     const bool inactive = c.is_demoed || c.just_respawned;

@@ -137,6 +137,12 @@ class OracleSim:
         m = np.ascontiguousarray(cmds, np.uint8)
         _check(lib().orc_step_with_commands(self.h, _ptr(c), ctrl_stride, _ptr(m), cmd_stride, ticks))
 
+    def step_with_device_commands(self, ctrl_ptr: int, ctrl_stride: int, cmd_ptr: int, cmd_stride: int, ticks: int):
+        """Pointers passed through as they are: device pointers for the reference's CUDA build
+        (librg_oracle_cuda.so), host pointers for its CPU build."""
+        _check(lib().orc_step_with_commands(self.h, ctypes.c_void_p(ctrl_ptr), ctrl_stride, ctypes.c_void_p(cmd_ptr),
+                                            cmd_stride, ticks))
+
     def _down(self, fn, n, nbytes):
         out = np.zeros((n, nbytes), np.uint8)
         _check(fn(self.h, _ptr(out), n))
