@@ -414,8 +414,16 @@ __global__ void __launch_bounds__(256) car_rays_kernel(CarTickArgs a, int t) {
     const int e = idx / a.max_cars;
     if (arena_idle(a, e)) return;
     const rg::CarState& car = a.cars[idx];
-    if (car.is_demoed) return;  // a demolished car's vehicle update casts no rays
-    rg::wheel_mesh_ray_ahead(car, a.car_cfgs[idx], arena_mesh(a.base, e), wheel, a.stages[idx].wheel_mesh[wheel]);
+    rg::CarStage& st = a.stages[idx];
+    if (car.is_demoed) {  // a demolished car's vehicle update casts no rays
+        st.wheel_meets_car[wheel] = 0;
+        return;
+    }
+    const int base = e * a.max_cars, count = a.base.env_car_count[e], slot = idx - base;
+    const uint32_t excluded = rg::wheel_ray_excluded_bodies(car, a.car_cfgs[idx], a.broadphase + e, slot, count);
+    rg::wheel_mesh_ray_ahead(car, a.car_cfgs[idx], arena_mesh(a.base, e), wheel,
+                             rg::WheelOthers{a.cars + base, a.car_cfgs + base, count, slot, excluded},
+                             st.wheel_mesh[wheel], st.wheel_meets_car[wheel]);
 }
 
 __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) {
@@ -426,8 +434,11 @@ __global__ void __launch_bounds__(256) car_vehicle_kernel(CarTickArgs a, int t) 
     if (arena_idle(a, e)) return;
     const int base = e * a.max_cars;
     const int count = a.base.env_car_count[e];
+    // the car's update runs here when no wheel of the arena meets another car, or when the sweep-box rule shows that
+    // no other car can be under its wheels nor it under theirs
     const bool free =
-        (rg::arena_free_cars(a.cars + base, a.car_cfgs + base, a.broadphase[e], count) >> (idx - base)) & 1u;
+        !rg::arena_wheels_meet_cars(a.stages + base, count) ||
+        ((rg::arena_free_cars(a.cars + base, a.car_cfgs + base, a.broadphase[e], count) >> (idx - base)) & 1u);
     a.stages[idx].in_car_thread = free ? 1u : 0u;
     // every car's ball contact geometry, before its vehicle update (it reads poses only)
     rg::car_ball_stage(a.base.balls[e], a.snaps[e].ball_vel_bt, a.cars[idx], a.car_cfgs[idx], a.base.tc,

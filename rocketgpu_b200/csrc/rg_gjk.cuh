@@ -476,7 +476,11 @@ struct Epa {
     SV sv_store[kEpaMaxVertices];
     Face fc[kEpaMaxFaces];
     int nextsv;
+    // The free faces: `stock` holds the faces given back (most recent first), `fresh` the first never-used slot.
+    // btGjkEpa2 links all faces into its stock at initialisation and takes the head; taking given-back faces first,
+    // then fresh slots in index order, hands out the same faces in the same order without touching all 128.
     List hull, stock;
+    int16_t fresh;
     const Gjk* gjk;
 
     RG_HD const SV& vtx(int16_t i) const { return i >= kEpaMaxVertices ? gjk->store[i - kEpaMaxVertices] : sv_store[i]; }
@@ -506,7 +510,7 @@ struct Epa {
         nextsv = 0;
         hull.root = stock.root = -1;
         hull.count = stock.count = 0;
-        for (int i = 0; i < kEpaMaxFaces; ++i) append(stock, static_cast<int16_t>(kEpaMaxFaces - i - 1));
+        fresh = 0;
     }
     RG_HDI bool getedgedist(int16_t face, int16_t a, int16_t b, float& dist) {
         const V3 aw = vtx(a).w, bw = vtx(b).w;
@@ -531,9 +535,14 @@ struct Epa {
         return false;
     }
     RG_HDI int16_t newface(int16_t a, int16_t b, int16_t c, bool forced) {
-        if (stock.root >= 0) {
-            const int16_t face = stock.root;
-            remove(stock, face);
+        if (stock.root >= 0 || fresh < kEpaMaxFaces) {
+            int16_t face;
+            if (stock.root >= 0) {
+                face = stock.root;
+                remove(stock, face);
+            } else {
+                face = fresh++;
+            }
             append(hull, face);
             Face& F = fc[face];
             F.pass = 0;
@@ -556,7 +565,7 @@ struct Epa {
             append(stock, face);
             return -1;
         }
-        status = stock.root >= 0 ? kEpaOutOfVertices : kEpaOutOfFaces;
+        status = kEpaOutOfFaces;
         return -1;
     }
     RG_HDI int16_t findbest() {

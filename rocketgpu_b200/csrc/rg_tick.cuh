@@ -1044,6 +1044,7 @@ struct CarStage {
     PadContacts pads;    // the car's pad contacts after its post-tick (pad_contacts_stage)
     uint32_t in_car_thread;  // this tick's vehicle update and stage ran in the car's own thread (arena_free_cars)
     RayHit wheel_mesh[4];    // the wheels' arena-mesh rays, cast ahead of the vehicle update (wheel_mesh_ray_ahead)
+    uint8_t wheel_meets_car[4];  // the wheel's ray meets another car's box (0 for a demolished car)
     BallCarScratch ball_manifold;  // the car/ball manifold after this tick's geometry (car_ball_stage)
     uint32_t ball_staged;          // ball_manifold holds this tick's update
 };
@@ -1461,6 +1462,16 @@ RG_HDI uint32_t arena_free_cars(const CarState* cars, const CarConfig* cfgs, con
     for (int i = 0; i < count && i < 8; ++i)
         if (reach[i] == 0u && !((under >> i) & 1u)) free |= 1u << i;
     return free;
+}
+
+// Whether any wheel ray of the arena's cars meets another car's box this tick (from the rays cast ahead). When none
+// does, no vehicle update pushes another car or sees one, and every car's update depends on the car alone.
+RG_HDI bool arena_wheels_meet_cars(const CarStage* stages, int count) {
+    uint32_t any = 0u;
+    for (int i = 0; i < count; ++i)
+        any |= stages[i].wheel_meets_car[0] | stages[i].wheel_meets_car[1] | stages[i].wheel_meets_car[2] |
+               stages[i].wheel_meets_car[3];
+    return any != 0u;
 }
 
 RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, Broadphase& bp, CarWorldScratch* cws,

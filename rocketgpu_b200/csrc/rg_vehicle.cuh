@@ -521,6 +521,43 @@ RG_HDI void wheel_mesh_ray(const WheelStep& w, const MeshDevice& mesh, float min
     }
 }
 
+// The closest of the other cars' boxes a wheel's suspension ray hits (best.hit = 0: none), skipping the cars the
+// broadphase excludes and demolished ones. It reads only the cars' poses, configs and demolition flags.
+RG_HDI void wheel_ray_vs_cars(const WheelStep& w, float min_hit_dist_sq_bt, const WheelOthers& oth, RayHit& best,
+                              int& best_idx, bool& best_nr) {
+    const float real_ray_length =
+        w.suspension_rest_length + w.max_suspension_travel + w.wheel_radius - kWheelSuspensionSubtraction;
+    const float real_ray_length_bt = (w.suspension_rest_length * kUuToBt + w.wheel_radius * kUuToBt) +
+                                     (w.max_suspension_travel - kWheelSuspensionSubtraction) * kUuToBt;
+    best.hit = 0;
+    best.t = 0.0f;
+    best_idx = -1;
+    best_nr = false;
+    for (int i = 0; i < oth.count; ++i) {
+        if (i == oth.self || ((oth.excluded >> (i + 1)) & 1u)) continue;
+        const CarState& o = oth.cars[i];
+        if (o.is_demoed) continue;
+        {
+            const CarConfig& ocfg = oth.cfgs[i];
+            const float reach = 0.5f * (fabs_(ocfg.hitbox_size.x) + fabs_(ocfg.hitbox_size.y) +
+                                        fabs_(ocfg.hitbox_size.z)) +
+                                fabs_(ocfg.hitbox_offset.x) + fabs_(ocfg.hitbox_offset.y) + fabs_(ocfg.hitbox_offset.z);
+            const float rr = reach * kUuToBt + real_ray_length_bt + 1.0e-2f;
+            if (len2(o.pos_bt - w.ray_source_bt) > rr * rr) continue;
+        }
+        RayHit h;
+        if (!wheel_ray_vs_car_box(w.ray_source_bt, w.wheel_dir_ws, real_ray_length, real_ray_length_bt, o, oth.cfgs[i],
+                                  h))
+            continue;
+        if (min_hit_dist_sq_bt > 0.0f && len2(h.point_bt - w.ray_source_bt) < min_hit_dist_sq_bt) continue;
+        if (!best.hit || h.t < best.t) {
+            best = h;
+            best_idx = i;
+            best_nr = o.demo_no_contact_response != 0;
+        }
+    }
+}
+
 // A wheel's suspension ray against the arena mesh (or its result `mesh_hit`, cast ahead by wheel_mesh_ray), the
 // other cars' boxes and the ball; the closest hit becomes the wheel's contact.
 RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& ball, const TickConfig& tc,
@@ -541,33 +578,9 @@ RG_HDI void wheel_ray_cast(const CarState& c, WheelStep& w, const BallState& bal
     bool selected_no_response = false;
     if (oth.cars) {
         RayHit best;
-        best.hit = 0;
-        best.t = 0.0f;
         int best_idx = -1;
         bool best_nr = false;
-        for (int i = 0; i < oth.count; ++i) {
-            if (i == oth.self || ((oth.excluded >> (i + 1)) & 1u)) continue;
-            const CarState& o = oth.cars[i];
-            if (o.is_demoed) continue;
-            {
-                const CarConfig& ocfg = oth.cfgs[i];
-                const float reach = 0.5f * (fabs_(ocfg.hitbox_size.x) + fabs_(ocfg.hitbox_size.y) +
-                                            fabs_(ocfg.hitbox_size.z)) +
-                                    fabs_(ocfg.hitbox_offset.x) + fabs_(ocfg.hitbox_offset.y) + fabs_(ocfg.hitbox_offset.z);
-                const float rr = reach * kUuToBt + real_ray_length_bt + 1.0e-2f;
-                if (len2(o.pos_bt - w.ray_source_bt) > rr * rr) continue;
-            }
-            RayHit h;
-            if (!wheel_ray_vs_car_box(w.ray_source_bt, w.wheel_dir_ws, real_ray_length, real_ray_length_bt, o,
-                                      oth.cfgs[i], h))
-                continue;
-            if (min_hit_dist_sq_bt > 0.0f && len2(h.point_bt - w.ray_source_bt) < min_hit_dist_sq_bt) continue;
-            if (!best.hit || h.t < best.t) {
-                best = h;
-                best_idx = i;
-                best_nr = o.demo_no_contact_response != 0;
-            }
-        }
+        wheel_ray_vs_cars(w, min_hit_dist_sq_bt, oth, best, best_idx, best_nr);
         if (best.hit && (!hit.hit || best.t < hit.t)) {
             hit = best;
             hit_world = false;
@@ -1317,14 +1330,23 @@ struct PreContactCar {
 };
 // Wheel `i`'s arena-mesh ray as the car's vehicle update casts it (the same wheel set-up from the car's pose and
 // config), for running the rays of every car ahead of the updates, one thread per wheel.
-RG_HDI void wheel_mesh_ray_ahead(const CarState& c, const CarConfig& cfg, const MeshDevice& mesh, int i, RayHit& hit) {
+// Also reports whether the ray meets another car's box (`oth`: the arena's cars with this car's broadphase
+// exclusions), which is when the update can push that car and must run in the arena's car order.
+RG_HDI void wheel_mesh_ray_ahead(const CarState& c, const CarConfig& cfg, const MeshDevice& mesh, int i,
+                                 const WheelOthers& oth, RayHit& hit, uint8_t& meets_car) {
     CarFrame f;
     car_basis(c, f.fwd, f.right, f.up);
     float front_bone, back_bone;
     wheel_bone_z(cfg, front_bone, back_bone);
     WheelStep w;
     init_wheel(w, c, cfg, i, f, i < 2 ? front_bone : back_bone);
-    wheel_mesh_ray(w, mesh, min_wheel_hit_dist_sq_bt(cfg), hit);
+    const float min_hit_dist_sq = min_wheel_hit_dist_sq_bt(cfg);
+    wheel_mesh_ray(w, mesh, min_hit_dist_sq, hit);
+    RayHit best;
+    int best_idx;
+    bool best_nr;
+    wheel_ray_vs_cars(w, min_hit_dist_sq, oth, best, best_idx, best_nr);
+    meets_car = best.hit ? 1 : 0;
 }
 
 RG_HDI void car_world_prestep(CarState& c, const CarConfig& cfg, const WheelRuntime& wr, const TickConfig& tc,
