@@ -680,15 +680,19 @@ def run_reference_cuda(args, world, rank):
     gen = w.controls()
     step_s = []
     for k in range(SETTLE_STEPS + args.warmup + args.steps):
+        timed = k >= SETTLE_STEPS + args.warmup
         ctrl_dev.copy_(torch.from_numpy(next(gen).reshape(-1)))
         cmd_dev.copy_(torch.from_numpy(cmds.reshape(-1)))
         flush.zero_()
         torch.cuda.synchronize()
+        if timed:
+            torch.cuda.nvtx.range_push("timed")
         t0 = time.perf_counter()
         sim.step_with_device_commands(ctrl_dev.data_ptr(), ENVS * MAX_CARS, cmd_dev.data_ptr(), ENVS, TICKS_PER_STEP)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        if k >= SETTLE_STEPS + args.warmup:
+        if timed:
+            torch.cuda.nvtx.range_pop()
             step_s.append(dt)
         cmds[:ENVS] = clock.commands(sim.envs(), sim.cars(), w.counts)
     final = (_active_car_rows(sim.cars(), w.counts), sim.balls())

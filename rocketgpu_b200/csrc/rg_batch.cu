@@ -398,7 +398,15 @@ __global__ void __launch_bounds__(256) car_pre_kernel(CarTickArgs a, int t) {
     rc.env_tick = a.base.envs[e].tick;
     rc.car_id = static_cast<uint32_t>(le * a.max_cars + (idx - e * a.max_cars) + 1);
     rc.team = a.teams[idx];
-    rg::car_tick_pre(a.cars[idx], ctrl, a.car_cfgs[idx], a.base.tc, a.wheels[idx], rc, a.records[idx]);
+    // the car's structs are worked on in local copies: one burst of independent loads, after which the warp's
+    // accesses to a field go to one interleaved local line instead of 32 lines of 880-byte-strided structs (measured:
+    // faster here, where the tick start touches most of the car; slower in the post-tick, which touches little)
+    rg::CarState car = a.cars[idx];
+    rg::WheelRuntime wr = a.wheels[idx];
+    const rg::CarConfig cfg = a.car_cfgs[idx];
+    rg::car_tick_pre(car, ctrl, cfg, a.base.tc, wr, rc, a.records[idx]);
+    a.cars[idx] = car;
+    a.wheels[idx] = wr;
 }
 
 // Tick part 3, one thread per active car: the vehicle update (four suspension rays against the arena mesh and the
