@@ -186,14 +186,38 @@ typedef struct rg_sim_config {
     uint8_t reserved[7];
 } rg_sim_config;
 
-/* A custom arena (reference ArenaLayout, rocketgpu.h:943-959): one triangle mesh in uu; pads, goals and spawns are
- * the official soccar ones. */
+/* reference ArenaSpawn (rocketgpu.h:929-933): pos.z is the ground under the car (its spawn_z is added); yaw in rad */
+typedef struct rg_arena_spawn { rg_vec3 pos; float yaw; } rg_arena_spawn;
+/* reference ArenaGoal (rocketgpu.h:935-942): the other team scores when the ball's centre is at least the ball radius
+ * past the plane through point (normal into the goal) and inside [min, max] */
+typedef struct rg_arena_goal { rg_vec3 point, normal, min, max; } rg_arena_goal;
+/* reference BoostPadConfig (rocketgpu.h:518-524) */
+typedef struct rg_boost_pad_config { rg_vec3 pos; uint8_t is_big, reserved0, reserved1, reserved2; } rg_boost_pad_config;
+/* The rules part of reference ArenaLayout (goals[2], kickoff_spawns[2][5], respawn_spawns[2][4], ball_spawn); teams
+ * index the arrays (0 blue, 1 orange). rg_default_arena_rules fills the official ones. */
+typedef struct rg_arena_rules {
+    rg_arena_goal goals[2];
+    rg_arena_spawn kickoff_spawns[2][5];
+    rg_arena_spawn respawn_spawns[2][4];
+    rg_vec3 ball_spawn;
+} rg_arena_rules;
+
+/* A custom arena (reference ArenaLayout, rocketgpu.h:943-959): one triangle mesh in uu, optional rules and pads.
+ * Rules equal to the official ones behave as null, as the reference's SameArenaRules test makes them
+ * (src/rocketgpu.cpp:834-849); positions are validated as ValidateArenaLayout does (finite, within 11,500 uu, spawn
+ * yaw within 8 pi, goal normal nonzero, goal bounds not NaN). Planes and mesh directories are not built. */
 typedef struct rg_arena_layout {
     const float* vertices_uu;   /* 3 * vertex_count */
     int64_t vertex_count;
     const int32_t* indices;     /* 3 per triangle */
     int64_t index_count;
+    const rg_arena_rules* rules;            /* null: the official goals, spawns and ball spawn */
+    const rg_boost_pad_config* boost_pads;  /* null: the 34 soccar pads */
+    int32_t boost_pad_count;                /* with boost_pads: 0..48 (reference kMaxBoostPads) */
+    int32_t reserved;
 } rg_arena_layout;
+/* The official rules (reference ArenaLayout::ArenaLayout, src/rocketgpu.cpp:2754-2775). */
+RG_API void rg_default_arena_rules(rg_arena_rules* out);
 
 typedef struct rg_batch rg_batch;
 

@@ -90,8 +90,19 @@ int orc_default_states(void* car, void* ball, void* env, void* pad, void* cfg) {
 
 // flags bit0: kickoff_settled (MutatorConfig::kickoff_settled); bit1: enable_boost_pads; bit2: car-car collisions;
 // bit3: demos; bit4: scoring.
+// rules_f (optional): 99 floats, goals[2] (point, normal, min, max), kickoff_spawns[2][5] (pos, yaw),
+// respawn_spawns[2][4] (pos, yaw), ball_spawn; pads_f (optional): pad_count x (x, y, z, is_big).
+int orc_create_layout(int32_t env_count, int32_t max_cars, const float* verts_uu, int64_t vert_count,
+                      const int32_t* indices, int64_t index_count, uint64_t respawn_seed, uint32_t flags,
+                      const float* rules_f, const float* pads_f, int32_t pad_count, void** out);
 int orc_create(int32_t env_count, int32_t max_cars, const float* verts_uu, int64_t vert_count, const int32_t* indices,
                int64_t index_count, uint64_t respawn_seed, uint32_t flags, void** out) {
+    return orc_create_layout(env_count, max_cars, verts_uu, vert_count, indices, index_count, respawn_seed, flags,
+                             nullptr, nullptr, 0, out);
+}
+int orc_create_layout(int32_t env_count, int32_t max_cars, const float* verts_uu, int64_t vert_count,
+                      const int32_t* indices, int64_t index_count, uint64_t respawn_seed, uint32_t flags,
+                      const float* rules_f, const float* pads_f, int32_t pad_count, void** out) {
     return Guard([&] {
         SimConfig cfg;
         cfg.env_count = env_count;
@@ -110,6 +121,34 @@ int orc_create(int32_t env_count, int32_t max_cars, const float* verts_uu, int64
         }
         mesh.indices.assign(indices, indices + index_count);
         layout.meshes.push_back(std::move(mesh));
+        if (rules_f) {
+            const float* f = rules_f;
+            auto v3 = [&]() { const Vec3 v(f[0], f[1], f[2]); f += 3; return v; };
+            for (int t = 0; t < 2; ++t) {
+                layout.goals[t].point = v3();
+                layout.goals[t].normal = v3();
+                layout.goals[t].min = v3();
+                layout.goals[t].max = v3();
+            }
+            for (int t = 0; t < 2; ++t)
+                for (int k = 0; k < 5; ++k) {
+                    layout.kickoff_spawns[t][k].pos = v3();
+                    layout.kickoff_spawns[t][k].yaw = *f++;
+                }
+            for (int t = 0; t < 2; ++t)
+                for (int k = 0; k < 4; ++k) {
+                    layout.respawn_spawns[t][k].pos = v3();
+                    layout.respawn_spawns[t][k].yaw = *f++;
+                }
+            layout.ball_spawn = v3();
+        }
+        if (pads_f) {
+            layout.boost_pads.resize((size_t)pad_count);
+            for (int32_t p = 0; p < pad_count; ++p) {
+                layout.boost_pads[(size_t)p].pos = Vec3(pads_f[4 * p], pads_f[4 * p + 1], pads_f[4 * p + 2]);
+                layout.boost_pads[(size_t)p].is_big = pads_f[4 * p + 3] != 0.0f ? 1 : 0;
+            }
+        }
         auto* o = new OracleSim;
         o->sim.reset(new BatchSim(cfg, layout));
         *out = o;

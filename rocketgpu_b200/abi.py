@@ -28,7 +28,7 @@ EXPORTS = [
     "rg_server_submit", "rg_server_poll", "rg_server_get_stats", "rg_batch_add_mesh", "rg_batch_set_arena_meshes",
     "rg_batch_set_launch_config", "rg_batch_get_launch_config", "rg_batch_upload_state_array",
     "rg_batch_download_state_array", "rg_batch_internal_state_layout", "rg_batch_download_internal_state",
-    "rg_batch_upload_internal_state", "rg_car_preset",
+    "rg_batch_upload_internal_state", "rg_car_preset", "rg_default_arena_rules",
 ]
 
 
@@ -48,9 +48,32 @@ class rg_sim_config(ctypes.Structure):
     ]
 
 
+class rg_vec3(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class rg_arena_spawn(ctypes.Structure):
+    _fields_ = [("pos", rg_vec3), ("yaw", ctypes.c_float)]
+
+
+class rg_arena_goal(ctypes.Structure):
+    _fields_ = [("point", rg_vec3), ("normal", rg_vec3), ("min", rg_vec3), ("max", rg_vec3)]
+
+
+class rg_boost_pad_config(ctypes.Structure):
+    _fields_ = [("pos", rg_vec3), ("is_big", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3)]
+
+
+class rg_arena_rules(ctypes.Structure):
+    _fields_ = [("goals", rg_arena_goal * 2), ("kickoff_spawns", (rg_arena_spawn * 5) * 2),
+                ("respawn_spawns", (rg_arena_spawn * 4) * 2), ("ball_spawn", rg_vec3)]
+
+
 class rg_arena_layout(ctypes.Structure):
     _fields_ = [("vertices_uu", ctypes.POINTER(ctypes.c_float)), ("vertex_count", ctypes.c_int64),
-                ("indices", ctypes.POINTER(ctypes.c_int32)), ("index_count", ctypes.c_int64)]
+                ("indices", ctypes.POINTER(ctypes.c_int32)), ("index_count", ctypes.c_int64),
+                ("rules", ctypes.POINTER(rg_arena_rules)), ("boost_pads", ctypes.POINTER(rg_boost_pad_config)),
+                ("boost_pad_count", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class rg_device_view(ctypes.Structure):
@@ -117,6 +140,7 @@ def lib():
         L.rg_default_car_state.argtypes = [vp]
         L.rg_default_car_config.argtypes = [vp]
         L.rg_car_preset.argtypes = [i32, vp]
+        L.rg_default_arena_rules.argtypes = [vp]
         L.rg_batch_pad_capacity.argtypes = [vp]
         L.rg_batch_pad_capacity.restype = i64
         L.rg_batch_step_with_device_controls.argtypes = [vp, vp, i32, i32, vp]

@@ -52,6 +52,14 @@ def car_preset(preset) -> np.ndarray:
     return out
 
 
+def arena_rules() -> "abi.rg_arena_rules":
+    """The official goals, kickoff / respawn spawns and ball spawn (reference ArenaLayout()), to edit field by field:
+    `r.goals[t].point.y`, `r.kickoff_spawns[t][k].pos`, `.yaw`, `r.respawn_spawns[t][k]`, `r.ball_spawn` (uu, rad)."""
+    r = abi.rg_arena_rules()
+    abi.lib().rg_default_arena_rules(ctypes.byref(r))
+    return r
+
+
 class SimConfig:
     """The reference SimConfig / MutatorConfig fields this path takes (defaults as the reference's)."""
 
@@ -73,7 +81,10 @@ class BatchSim:
     `vertices` (float32 [V, 3], uu) and `indices` (int32 [3T]) are the arena's triangle mesh (ArenaLayout.meshes[0]).
     """
 
-    def __init__(self, config: SimConfig, vertices: np.ndarray, indices: np.ndarray, device: int = 0):
+    def __init__(self, config: SimConfig, vertices: np.ndarray, indices: np.ndarray, device: int = 0,
+                 rules: "abi.rg_arena_rules | None" = None, boost_pads=None):
+        """`rules`: the layout's goals and spawns (arena_rules(), edited), None for the official ones;
+        `boost_pads`: [(x, y, z, is_big)] (at most 48), None for the 34 soccar pads."""
         self._v = np.ascontiguousarray(vertices, np.float32)
         self._i = np.ascontiguousarray(indices, np.int32)
         lay = abi.rg_arena_layout()
@@ -81,6 +92,16 @@ class BatchSim:
         lay.vertex_count = len(self._v)
         lay.indices = self._i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
         lay.index_count = len(self._i)
+        if rules is not None:
+            self._rules = rules
+            lay.rules = ctypes.pointer(rules)
+        if boost_pads is not None:
+            self._pads = (abi.rg_boost_pad_config * max(1, len(boost_pads)))()
+            for k, (x, y, z, big) in enumerate(boost_pads):
+                self._pads[k].pos = abi.rg_vec3(x, y, z)
+                self._pads[k].is_big = int(big)
+            lay.boost_pads = ctypes.cast(self._pads, ctypes.POINTER(abi.rg_boost_pad_config))
+            lay.boost_pad_count = len(boost_pads)
         h = ctypes.c_void_p()
         _check(abi.lib().rg_batch_create(ctypes.byref(config.c), ctypes.byref(lay), device, ctypes.byref(h)))
         self._h = h

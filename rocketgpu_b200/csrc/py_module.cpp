@@ -47,6 +47,9 @@ struct ArenaMesh {
 
 struct ArenaLayout {
     std::vector<ArenaMesh> meshes;
+    std::vector<rg_boost_pad_config> boost_pads;  // empty: the 34 soccar pads
+    rg_arena_rules rules;
+    ArenaLayout() { rg_default_arena_rules(&rules); }
 };
 
 class BatchSim {
@@ -56,6 +59,11 @@ class BatchSim {
         const ArenaMesh& m = layout.meshes[0];
         rg_arena_layout l{m.vertices.data(), static_cast<int64_t>(m.vertices.size() / 3), m.indices.data(),
                           static_cast<int64_t>(m.indices.size())};
+        l.rules = &layout.rules;
+        if (!layout.boost_pads.empty()) {
+            l.boost_pads = layout.boost_pads.data();
+            l.boost_pad_count = static_cast<int32_t>(layout.boost_pads.size());
+        }
         check(rg_batch_create(&cfg, &l, device, &b_));
         cfg_ = cfg;
     }
@@ -206,7 +214,74 @@ PYBIND11_MODULE(rocketgpu_py_b200, m) {
              py::arg("vertices"), py::arg("indices"))
         .def_readwrite("vertices", &ArenaMesh::vertices)
         .def_readwrite("indices", &ArenaMesh::indices);
-    py::class_<ArenaLayout>(m, "ArenaLayout").def(py::init<>()).def_readwrite("meshes", &ArenaLayout::meshes);
+    py::class_<rg_vec3>(m, "Vec3")
+        .def(py::init([](float x, float y, float z) { return rg_vec3{x, y, z}; }), py::arg("x") = 0.0f,
+             py::arg("y") = 0.0f, py::arg("z") = 0.0f)
+        .def_readwrite("x", &rg_vec3::x)
+        .def_readwrite("y", &rg_vec3::y)
+        .def_readwrite("z", &rg_vec3::z);
+    py::class_<rg_arena_spawn>(m, "ArenaSpawn")
+        .def(py::init([](rg_vec3 pos, float yaw) { return rg_arena_spawn{pos, yaw}; }), py::arg("pos") = rg_vec3{},
+             py::arg("yaw") = 0.0f)
+        .def_readwrite("pos", &rg_arena_spawn::pos)
+        .def_readwrite("yaw", &rg_arena_spawn::yaw);
+    py::class_<rg_arena_goal>(m, "ArenaGoal")
+        .def(py::init([]() { rg_arena_rules r; rg_default_arena_rules(&r); return r.goals[1]; }))
+        .def_readwrite("point", &rg_arena_goal::point)
+        .def_readwrite("normal", &rg_arena_goal::normal)
+        .def_readwrite("min", &rg_arena_goal::min)
+        .def_readwrite("max", &rg_arena_goal::max);
+    py::class_<rg_boost_pad_config>(m, "BoostPadConfig")
+        .def(py::init([](rg_vec3 pos, bool is_big) {
+                 rg_boost_pad_config c{};
+                 c.pos = pos;
+                 c.is_big = is_big ? 1 : 0;
+                 return c;
+             }),
+             py::arg("pos") = rg_vec3{}, py::arg("is_big") = false)
+        .def_readwrite("pos", &rg_boost_pad_config::pos)
+        .def_readwrite("is_big", &rg_boost_pad_config::is_big);
+    // the rules part is read and written whole (lists of copies), as the reference binding's arrays are
+    py::class_<ArenaLayout>(m, "ArenaLayout")
+        .def(py::init<>())
+        .def_readwrite("meshes", &ArenaLayout::meshes)
+        .def_readwrite("boost_pads", &ArenaLayout::boost_pads)
+        .def_property(
+            "goals", [](const ArenaLayout& l) { return std::vector<rg_arena_goal>{l.rules.goals[0], l.rules.goals[1]}; },
+            [](ArenaLayout& l, const std::vector<rg_arena_goal>& g) {
+                if (g.size() != 2) throw py::value_error("goals: two goals (blue, orange)");
+                l.rules.goals[0] = g[0];
+                l.rules.goals[1] = g[1];
+            })
+        .def_property(
+            "kickoff_spawns",
+            [](const ArenaLayout& l) {
+                std::vector<std::vector<rg_arena_spawn>> out(2);
+                for (int t = 0; t < 2; ++t) out[t].assign(l.rules.kickoff_spawns[t], l.rules.kickoff_spawns[t] + 5);
+                return out;
+            },
+            [](ArenaLayout& l, const std::vector<std::vector<rg_arena_spawn>>& v) {
+                if (v.size() != 2 || v[0].size() != 5 || v[1].size() != 5)
+                    throw py::value_error("kickoff_spawns: 2 teams x 5 spawns");
+                for (int t = 0; t < 2; ++t)
+                    for (int k = 0; k < 5; ++k) l.rules.kickoff_spawns[t][k] = v[t][k];
+            })
+        .def_property(
+            "respawn_spawns",
+            [](const ArenaLayout& l) {
+                std::vector<std::vector<rg_arena_spawn>> out(2);
+                for (int t = 0; t < 2; ++t) out[t].assign(l.rules.respawn_spawns[t], l.rules.respawn_spawns[t] + 4);
+                return out;
+            },
+            [](ArenaLayout& l, const std::vector<std::vector<rg_arena_spawn>>& v) {
+                if (v.size() != 2 || v[0].size() != 4 || v[1].size() != 4)
+                    throw py::value_error("respawn_spawns: 2 teams x 4 spawns");
+                for (int t = 0; t < 2; ++t)
+                    for (int k = 0; k < 4; ++k) l.rules.respawn_spawns[t][k] = v[t][k];
+            })
+        .def_property(
+            "ball_spawn", [](const ArenaLayout& l) { return l.rules.ball_spawn; },
+            [](ArenaLayout& l, rg_vec3 v) { l.rules.ball_spawn = v; });
     py::class_<BatchSim>(m, "BatchSim")
         .def(py::init<const rg_sim_config&, const ArenaLayout&, int>(), py::arg("config"), py::arg("layout"),
              py::arg("device") = 0)

@@ -114,6 +114,7 @@ struct rg_batch {
     DeviceArray<int32_t> active_cars;
     int32_t active_car_count = 0;
     rg::PadLayout pad_layout{};
+    DeviceArray<rg::ArenaRules> rules;  // a custom layout's spawns and goals (b->tc.rules points here), or empty
     // Pads stay at their initial state until a car exists or pads are uploaded; until then ball-only arenas skip them.
     bool pads_live = false;
     rg::MeshHost mesh_host;
@@ -910,6 +911,104 @@ RG_API void rg_default_car_config(rg_car_config* o) {
     o->spawn_z = 36.02f;
 }
 
+// ---- the layout's rules and pads (reference ArenaLayout handling, src/rocketgpu.cpp:792-881, 1502-1536) ----------
+namespace {
+constexpr float kLayoutMaxCoord = 11500.0f;   // reference kArenaLayoutMaxCoord
+constexpr float kLayoutMaxYaw = 25.132741f;   // reference kArenaLayoutMaxYaw (8 pi)
+constexpr int kMaxLayoutPads = 48;            // reference kMaxBoostPads
+void check_position(const rg_vec3& v, const char* what) {
+    const bool ok = std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z) && std::fabs(v.x) <= kLayoutMaxCoord &&
+                    std::fabs(v.y) <= kLayoutMaxCoord && std::fabs(v.z) <= kLayoutMaxCoord;
+    if (!ok)
+        throw std::invalid_argument(std::string("ArenaLayout: ") + what +
+                                    " must be finite and within kArenaLayoutMaxCoord (11500 uu) of the origin on every axis");
+}
+bool same_vec(const rg_vec3& a, const rg_vec3& b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+// reference ValidateArenaLayout (rules and pads part) and SameArenaRules
+void validate_rules(const rg_arena_rules& r) {
+    for (int t = 0; t < 2; ++t) {
+        const rg_arena_goal& g = r.goals[t];
+        check_position(g.point, "a goal point");
+        if (!(std::isfinite(g.normal.x) && std::isfinite(g.normal.y) && std::isfinite(g.normal.z)))
+            throw std::invalid_argument("ArenaLayout: a goal normal must be finite");
+        for (const float x : {g.min.x, g.min.y, g.min.z, g.max.x, g.max.y, g.max.z})
+            if (std::isnan(x)) throw std::invalid_argument("ArenaLayout: a goal's min and max must not be NaN");
+        for (const rg_arena_spawn& sp : r.kickoff_spawns[t]) {
+            check_position(sp.pos, "a kickoff spawn position");
+            if (!(std::fabs(sp.yaw) <= kLayoutMaxYaw))
+                throw std::invalid_argument("ArenaLayout: a kickoff spawn yaw must be within 8 pi of zero");
+        }
+        for (const rg_arena_spawn& sp : r.respawn_spawns[t]) {
+            check_position(sp.pos, "a respawn spawn position");
+            if (!(std::fabs(sp.yaw) <= kLayoutMaxYaw))
+                throw std::invalid_argument("ArenaLayout: a respawn spawn yaw must be within 8 pi of zero");
+        }
+    }
+    check_position(r.ball_spawn, "the ball spawn");
+}
+bool same_rules(const rg_arena_rules& a, const rg_arena_rules& b) {
+    bool same = same_vec(a.ball_spawn, b.ball_spawn);
+    for (int t = 0; t < 2; ++t) {
+        same = same && same_vec(a.goals[t].point, b.goals[t].point) && same_vec(a.goals[t].normal, b.goals[t].normal) &&
+               same_vec(a.goals[t].min, b.goals[t].min) && same_vec(a.goals[t].max, b.goals[t].max);
+        for (int k = 0; k < 5; ++k)
+            same = same && same_vec(a.kickoff_spawns[t][k].pos, b.kickoff_spawns[t][k].pos) &&
+                   a.kickoff_spawns[t][k].yaw == b.kickoff_spawns[t][k].yaw;
+        for (int k = 0; k < 4; ++k)
+            same = same && same_vec(a.respawn_spawns[t][k].pos, b.respawn_spawns[t][k].pos) &&
+                   a.respawn_spawns[t][k].yaw == b.respawn_spawns[t][k].yaw;
+    }
+    return same;
+}
+// reference MakeArenaRules: goal normals normalized
+rg::ArenaRules make_rules(const rg_arena_rules& in) {
+    rg::ArenaRules r{};
+    auto v3 = [](const rg_vec3& v) { return rg::V3{v.x, v.y, v.z}; };
+    for (int t = 0; t < 2; ++t) {
+        for (int k = 0; k < 5; ++k) {
+            r.kickoff_pos[t][k] = v3(in.kickoff_spawns[t][k].pos);
+            r.kickoff_yaw[t][k] = in.kickoff_spawns[t][k].yaw;
+        }
+        for (int k = 0; k < 4; ++k) {
+            r.respawn_pos[t][k] = v3(in.respawn_spawns[t][k].pos);
+            r.respawn_yaw[t][k] = in.respawn_spawns[t][k].yaw;
+        }
+        const rg_arena_goal& g = in.goals[t];
+        const float len = std::sqrt((g.normal.x * g.normal.x + g.normal.y * g.normal.y) + g.normal.z * g.normal.z);
+        if (!(len > 0.0f) || !std::isfinite(len)) throw std::invalid_argument("ArenaGoal normal must be nonzero");
+        r.goal_point[t] = v3(g.point);
+        r.goal_normal[t] = rg::V3{g.normal.x / len, g.normal.y / len, g.normal.z / len};
+        r.goal_min[t] = v3(g.min);
+        r.goal_max[t] = v3(g.max);
+    }
+    r.ball_spawn = v3(in.ball_spawn);
+    return r;
+}
+}  // namespace
+
+RG_API void rg_default_arena_rules(rg_arena_rules* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    rg_sim_config c;
+    rg_sim_config_default(&c);
+    const float thr = c.goal_base_threshold_y;
+    o->goals[0] = rg_arena_goal{{0.0f, -thr, 0.0f}, {0.0f, -1.0f, 0.0f}, {-1.0e30f, -1.0e30f, -1.0e30f},
+                                {1.0e30f, 1.0e30f, 1.0e30f}};
+    o->goals[1] = rg_arena_goal{{0.0f, thr, 0.0f}, {0.0f, 1.0f, 0.0f}, {-1.0e30f, -1.0e30f, -1.0e30f},
+                                {1.0e30f, 1.0e30f, 1.0e30f}};
+    for (int k = 0; k < 5; ++k) {
+        const rg::SpawnPos sp = rg::soccar_kickoff_spawn(k);
+        o->kickoff_spawns[0][k] = rg_arena_spawn{{sp.x, sp.y, 0.0f}, sp.yaw};
+        o->kickoff_spawns[1][k] = rg_arena_spawn{{-sp.x, -sp.y, 0.0f}, sp.yaw + rg::kPiF};
+    }
+    for (int k = 0; k < 4; ++k) {
+        const rg::SpawnPos sp = rg::soccar_respawn_spawn(k);
+        o->respawn_spawns[0][k] = rg_arena_spawn{{sp.x, sp.y, 0.0f}, sp.yaw};
+        o->respawn_spawns[1][k] = rg_arena_spawn{{sp.x, -sp.y, 0.0f}, sp.yaw + rg::kPiF};
+    }
+    o->ball_spawn = rg_vec3{0.0f, 0.0f, 92.75f};
+}
+
 // The game's hitbox presets (reference OctaneConfig .. MercConfig, src/rocketgpu.cpp:417-490): hitbox (published size
 // + 2.5 uu per axis), offsets, wheel radii and suspension rest lengths, steering curves, spawn height, body id. The
 // numbers are the game's car data, the same in every implementation.
@@ -983,6 +1082,14 @@ RG_API int rg_car_preset(int32_t preset, rg_car_config* out) {
 RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layout, int device, rg_batch** out) {
     return guard([&] {
         if (!cfg || !layout || !out) throw std::invalid_argument("null argument");
+        if (layout->boost_pads) {
+            if (layout->boost_pad_count < 0 || layout->boost_pad_count > kMaxLayoutPads)
+                throw std::invalid_argument("ArenaLayout::boost_pads holds at most kMaxBoostPads pads");
+            for (int p = 0; p < layout->boost_pad_count; ++p) check_position(layout->boost_pads[p].pos, "a boost pad position");
+        } else if (layout->boost_pad_count != 0) {
+            throw std::invalid_argument("boost_pad_count without boost_pads");
+        }
+        if (layout->rules) validate_rules(*layout->rules);
         if (cfg->env_count <= 0) throw std::invalid_argument("env_count must be positive");
         // The car-car pair rows are sized for the 15 pairs of six cars (rg_car_car.cuh kMaxPairRows); 7- and 8-car
         // arenas would need more, so they are refused rather than run with rows dropped.
@@ -1031,12 +1138,31 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
                 b->pad_layout.pos[p] = rg::V3{kPads[p][0], kPads[p][1], kPads[p][2]};
                 b->pad_layout.is_big[p] = p >= 28 ? 1 : 0;
             }
+            if (layout->boost_pads) {  // the layout's own pads
+                b->pad_layout.count = layout->boost_pad_count;
+                for (int p = 0; p < layout->boost_pad_count; ++p) {
+                    const rg_boost_pad_config& pc = layout->boost_pads[p];
+                    b->pad_layout.pos[p] = rg::V3{pc.pos.x, pc.pos.y, pc.pos.z};
+                    b->pad_layout.is_big[p] = pc.is_big;
+                }
+            }
+            b->tc.pad_count = b->pad_layout.count;
+        }
+        if (layout->rules) {
+            rg_arena_rules official;
+            rg_default_arena_rules(&official);
+            if (!same_rules(*layout->rules, official)) {
+                const rg::ArenaRules r = make_rules(*layout->rules);
+                b->rules.alloc(1);
+                check(cudaMemcpy(b->rules.ptr, &r, sizeof(r), cudaMemcpyHostToDevice), "arena rules");
+                b->tc.rules = b->rules.ptr;
+            }
         }
         b->cars.alloc(cap);
         b->wheels.alloc(cap);
         b->car_cfgs.alloc(cap);
         b->controls.alloc(cap);
-        b->pads.alloc(static_cast<size_t>(b->env_count) * 34);
+        b->pads.alloc(static_cast<size_t>(b->env_count) * static_cast<size_t>(b->pad_layout.count));
         b->teams.alloc(cap);
         if (cap) check(cudaMemset(b->teams.ptr, 0, cap), "teams");
         b->broadphase.alloc(b->env_count);
@@ -1080,9 +1206,10 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
             check(cudaMemset(b->controls.ptr, 0, cap * sizeof(rg::CarControls)), "controls");
         }
         {
-            std::vector<rg::PadState> pads(static_cast<size_t>(b->env_count) * 34);
+            const size_t per = static_cast<size_t>(b->pad_layout.count);
+            std::vector<rg::PadState> pads(static_cast<size_t>(b->env_count) * per);
             for (size_t i = 0; i < pads.size(); ++i) {
-                pads[i] = rg::PadState{0.0f, 1, static_cast<uint8_t>((i % 34) >= 28 ? 1 : 0), 32768, 0, 0};
+                pads[i] = rg::PadState{0.0f, 1, b->pad_layout.is_big[i % per], 32768, 0, 0};
             }
             check(cudaMemcpy(b->pads.ptr, pads.data(), pads.size() * sizeof(rg::PadState), cudaMemcpyHostToDevice),
                   "pads");
@@ -1243,7 +1370,9 @@ RG_API int rg_batch_download_car_states(rg_batch* b, rg_car_state* host, size_t 
                        "download_car_states", stream);
     });
 }
-RG_API int64_t rg_batch_pad_capacity(const rg_batch* b) { return b ? static_cast<int64_t>(b->env_count) * 34 : 0; }
+RG_API int64_t rg_batch_pad_capacity(const rg_batch* b) {
+    return b ? static_cast<int64_t>(b->env_count) * b->pad_layout.count : 0;
+}
 RG_API int rg_batch_upload_pad_states(rg_batch* b, const rg_boost_pad_state* host, size_t count, void* stream) {
     return guard([&] {
         upload_array(b, b->pads, host, count, static_cast<size_t>(rg_batch_pad_capacity(b)), "upload_pad_states",

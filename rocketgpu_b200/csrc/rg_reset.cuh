@@ -139,8 +139,16 @@ RG_HDI void place_car_at_kickoff_spawn(CarState& c, int team, SpawnPos spawn, fl
     reset_car_common(c, boost);
 }
 
-// reference ResetBall(ball, Soccar, game_spawn = false) (arena_ball.hpp:2775-2815)
-RG_HDI void reset_kickoff_ball(BallState& b) {
+// reference PlaceCarAtWorldSpawn (arena_ball.hpp:2579-2585): a custom arena's spawn, pos.z the ground
+RG_HDI void place_car_at_world_spawn(CarState& c, V3 pos, float yaw, float z, float boost) {
+    car_set_pos_bt(c, V3{pos.x, pos.y, pos.z + z} * kUuToBt);
+    c.rot = quat_from_yaw(wrap_angle(yaw));
+    seed_car_basis_from_spawn(c, spawn_yaw_rotator_units(yaw), false);
+    reset_car_common(c, boost);
+}
+
+// reference ResetBall(ball, Soccar, game_spawn = false, rules) (arena_ball.hpp:2775-2815)
+RG_HDI void reset_kickoff_ball(BallState& b, const ArenaRules* rules = nullptr) {
     b.pos_bt = V3{0.0f, 0.0f, 93.15f} * kUuToBt;
     b.pos = b.pos_bt * 50.0f;
     b.rot = Q4{1.0f, 0.0f, 0.0f, 0.0f};
@@ -166,7 +174,8 @@ RG_HDI void reset_kickoff_ball(BallState& b) {
     b.sleeping = 0;
     b.deactivation_time = 0.0f;
     b.constrained_2d = 0;
-    b.pos_bt = V3{0.0f, 0.0f, 92.75f} * kUuToBt;
+    const V3 p = rules ? rules->ball_spawn : V3{0.0f, 0.0f, 92.75f};
+    b.pos_bt = V3{p.x, p.y, p.z} * kUuToBt;
     b.pos = b.pos_bt * 50.0f;
     b.sleeping = 1;
 }
@@ -183,12 +192,13 @@ RG_HDI bool kickoff_spot_preferred(SpawnPos a, SpawnPos b) {
     if (left_a != left_b) return left_a;
     return (a.y < 0.0f ? -a.y : a.y) > (b.y < 0.0f ? -b.y : b.y);
 }
-RG_HDI void prefer_kickoff_spot_for_short_team(int* order, int team_count) {
+// `spots`: the five kickoff spots of the blue side (a custom arena's blue kickoff positions, yaw unused)
+RG_HDI void prefer_kickoff_spot_for_short_team(int* order, int team_count, const SpawnPos* spots) {
     constexpr int kMaxTeamSize = 4;
     if (team_count <= 0 || team_count >= kMaxTeamSize) return;
     int best = 0;
     for (int i = 1; i < kMaxTeamSize; ++i)
-        if (kickoff_spot_preferred(soccar_kickoff_spawn(order[i]), soccar_kickoff_spawn(order[best]))) best = i;
+        if (kickoff_spot_preferred(spots[order[i]], spots[order[best]])) best = i;
     if (best < team_count) return;
     const int spot = order[best];
     order[best] = order[team_count - 1];
@@ -277,16 +287,21 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
     }
     int team_order[2][5];
     for (int j = 0; j < 5; ++j) team_order[0][j] = team_order[1][j] = kickoff_order[j];
+    const ArenaRules* rules = tc.rules;
     if (next_kickoff && blue_count != orange_count) {
+        SpawnPos spots[5];
+        for (int i = 0; i < 5; ++i)
+            spots[i] = rules ? SpawnPos{rules->kickoff_pos[0][i].x, rules->kickoff_pos[0][i].y, 0.0f}
+                             : soccar_kickoff_spawn(i);
         const int short_team = blue_count < orange_count ? 0 : 1;
-        prefer_kickoff_spot_for_short_team(team_order[short_team], short_team == 0 ? blue_count : orange_count);
+        prefer_kickoff_spot_for_short_team(team_order[short_team], short_team == 0 ? blue_count : orange_count, spots);
     }
     env = next;
     uint32_t order_bits[2] = {0, 0};
     for (int t = 0; t < 2; ++t)
         for (int i = 0; i < 5; ++i) order_bits[t] |= static_cast<uint32_t>(team_order[t][i]) << (3 * i);
 
-    reset_kickoff_ball(ball);
+    reset_kickoff_ball(ball, rules);
     if (pads && !how.keep_pads) {
         for (int p = 0; p < L.count; ++p) {
             PadState& pad = pads[p];
@@ -314,6 +329,17 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
         }
         if (!found) continue;
         const int spot = nth < 5 ? static_cast<int>((order_bits[team == 0 ? 0 : 1] >> (3 * nth)) & 7u) : nth;
+        if (rules) {
+            // a custom arena's spots (reference PlaceKickoffCar with ArenaRules, arena_ball.hpp:2998-3007)
+            const int t = team == 0 ? 0 : 1;
+            const int r = (nth - 5) % 4;
+            const float step = 250.0f * static_cast<float>((nth - 5) / 4);
+            V3 pos = nth < 5 ? rules->kickoff_pos[t][spot] : rules->respawn_pos[t][r];
+            const float yaw = nth < 5 ? rules->kickoff_yaw[t][spot] : rules->respawn_yaw[t][r];
+            if (nth >= 5) pos = pos - V3{game_cosf(yaw), game_sinf(yaw), 0.0f} * step;
+            place_car_at_world_spawn(cars[i], pos, yaw, cfgs[i].spawn_z, tc.boost_spawn_amount);
+            continue;
+        }
         SpawnPos spawn;
         if (nth >= 5) {
             // a sixth car of a team takes a respawn spot, 250 uu further back per round of four

@@ -58,6 +58,18 @@ static_assert(offsetof(EnvState, frame_frac_prev) == offsetof(rg_env_state, fram
 
 // Constants of one BatchSim config, resolved on the host (the reference's SimConfig + MutatorConfig fields the tick
 // reads, with BatchSim's derived values such as the cached per-tick drag factor).
+// A custom arena's spawns, ball spawn and goals (reference ArenaRules, detail/constants.hpp:57-67, made by
+// MakeArenaRules, src/rocketgpu.cpp:859-881: goal normals normalized). TickConfig::rules points at one when the
+// layout's rules differ from the official ones; null otherwise.
+struct ArenaRules {
+    V3 kickoff_pos[2][5];
+    float kickoff_yaw[2][5];
+    V3 respawn_pos[2][4];
+    float respawn_yaw[2][4];
+    V3 ball_spawn;
+    V3 goal_point[2], goal_normal[2], goal_min[2], goal_max[2];
+};
+
 struct TickConfig {
     float tick_dt;
     float gravity_z;
@@ -87,6 +99,7 @@ struct TickConfig {
     uint8_t enable_car_car, enable_demos, enable_team_demos;
     float bump_force_scale, bump_cooldown_time;
     uint64_t kickoff_seed;  // the last reset_to_kickoff seed: demolished cars' respawn draw (reference Impl::seed)
+    const ArenaRules* rules;  // custom spawns and goals (memory the kernels can read), or null
 };
 
 }  // namespace rg

@@ -138,7 +138,27 @@ RG_HDI void ball_finish(BallState& b) {
 // CountdownUpdateTimers :6516-6537). The countdown's end re-enables driving of the arena's first `count` car slots.
 RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState* cars = nullptr, int count = 0) {
     ball_finish(b);
-    if (c.enable_scoring) {
+    if (c.enable_scoring && c.rules) {
+        // a custom arena's goals (reference ScoreArenaRulesGoals, env_step.hpp:6951-6966)
+        const ArenaRules& R = *c.rules;
+        for (int t = 0; t < 2; ++t) {
+            const V3 lo = R.goal_min[t], hi = R.goal_max[t];
+            if (dot(b.pos - R.goal_point[t], R.goal_normal[t]) >= c.ball_radius && b.pos.x >= lo.x && b.pos.y >= lo.y &&
+                b.pos.z >= lo.z && b.pos.x <= hi.x && b.pos.y <= hi.y && b.pos.z <= hi.z) {
+                const int scorer = t == 0 ? 1 : 0;  // the blue goal (0) scores for orange
+                env.last_scored_team = scorer;
+                env.goal_scored_this_tick = 1;
+                if (!env.goal_latched) {
+                    if (scorer == 0)
+                        env.blue_score += 1;
+                    else
+                        env.orange_score += 1;
+                }
+                break;
+            }
+        }
+        env.goal_latched = env.goal_scored_this_tick;
+    } else if (c.enable_scoring) {
         const float score_threshold = c.goal_base_threshold_y + c.ball_radius;
         if (b.pos.y >= score_threshold) {
             env.last_scored_team = 0;
@@ -348,6 +368,39 @@ RG_HDI void respawn_car(CarState& c, const CarConfig& cfg, const TickConfig& tc,
         c.respawn_slot_override_plus1 = 0;
     }
     if (slot < 0) slot = respawn_start_index(rc.seed, rc.env_idx, static_cast<uint64_t>(rc.env_tick), rc.car_id);
+    if (tc.rules) {
+        // a custom arena's spots (reference KickoffSpawnCar / RespawnCar / RespawnPlace with ArenaRules,
+        // arena_ball.hpp:3098-3160)
+        const ArenaRules& R = *tc.rules;
+        const int t = team == 0 ? 0 : 1;
+        if (offset_dir < 0 && slot >= kKickoffSpawnOverridePlus1 - 1) {
+            const int spot = slot - (kKickoffSpawnOverridePlus1 - 1);
+            const int ks = spot >= 0 && spot < 4 ? spot : 4;
+            const uint16_t driving_disabled = c.driving_disabled;
+            place_car_at_world_spawn(c, R.kickoff_pos[t][ks], R.kickoff_yaw[t][ks], cfg.spawn_z, tc.boost_spawn_amount);
+            c.driving_disabled = driving_disabled;
+            c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
+            return;
+        }
+        const int rs = (slot % 4) & 3;
+        V3 ground = R.respawn_pos[t][rs];
+        const float yaw = R.respawn_yaw[t][rs];
+        if (offset_dir >= 0) {
+            const Q4 q = quat_from_yaw(wrap_angle(yaw));
+            const float fx = q.w * q.w - q.z * q.z;
+            const float fy = 2.0f * q.w * q.z;
+            constexpr float k = 0.70710677f;
+            const int d = offset_dir & 7;
+            const float ux = d == 0 ? 1.0f : (d == 1 || d == 7) ? k : (d == 2 || d == 6) ? 0.0f : (d == 3 || d == 5) ? -k : -1.0f;
+            const float uy = (d == 0 || d == 4) ? 0.0f : (d == 1 || d == 3) ? k : d == 2 ? 1.0f : d == 6 ? -1.0f : -k;
+            ground.x += 192.0f * (fx * ux - fy * uy);
+            ground.y += 192.0f * (fx * uy + fy * ux);
+        }
+        place_car_at_world_spawn(c, ground, yaw, cfg.spawn_z, tc.boost_spawn_amount);
+        c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
+        c.is_on_ground = 0;
+        return;
+    }
     if (offset_dir < 0 && slot >= kKickoffSpawnOverridePlus1 - 1) {
         const uint16_t driving_disabled = c.driving_disabled;
         place_car_at_kickoff_spawn(c, team, soccar_kickoff_spawn(slot - (kKickoffSpawnOverridePlus1 - 1)), cfg.spawn_z,

@@ -30,6 +30,7 @@ def lib():
         L.orc_last_error.restype = ctypes.c_char_p
         L.orc_create.argtypes = [i32, i32, vp, i64, vp, i64, ctypes.c_uint64, ctypes.c_uint32,
                                  ctypes.POINTER(vp)]
+        L.orc_create_layout.argtypes = [i32, i32, vp, i64, vp, i64, ctypes.c_uint64, ctypes.c_uint32, vp, vp, i32, vp]
         L.orc_destroy.argtypes = [vp]
         L.orc_car_capacity.argtypes = [vp]
         L.orc_car_capacity.restype = i64
@@ -81,14 +82,19 @@ class OracleSim:
 
     def __init__(self, env_count: int, max_cars: int, vertices: np.ndarray, indices: np.ndarray,
                  respawn_seed: int = 0, kickoff_settled: bool = True, boost_pads: bool = True,
-                 car_car: bool = True, demos: bool = True, scoring: bool = True):
+                 car_car: bool = True, demos: bool = True, scoring: bool = True, rules=None, pad_layout=None):
+        """`rules`: 99 floats in rg_arena_rules order (goals, kickoff spawns, respawn spawns, ball spawn);
+        `pad_layout`: [(x, y, z, is_big)] replacing the 34 soccar pads."""
         v = np.ascontiguousarray(vertices, np.float32)
         i = np.ascontiguousarray(indices, np.int32)
         flags = (1 if kickoff_settled else 0) | (2 if boost_pads else 0) | (4 if car_car else 0) | \
             (8 if demos else 0) | (16 if scoring else 0)
         h = ctypes.c_void_p()
-        _check(lib().orc_create(env_count, max_cars, _ptr(v), len(v), _ptr(i), len(i), respawn_seed, flags,
-                                ctypes.byref(h)))
+        rf = None if rules is None else np.ascontiguousarray(rules, np.float32).reshape(99)
+        pf = None if pad_layout is None else np.ascontiguousarray(pad_layout, np.float32).reshape(-1, 4)
+        _check(lib().orc_create_layout(env_count, max_cars, _ptr(v), len(v), _ptr(i), len(i), respawn_seed, flags,
+                                       None if rf is None else _ptr(rf), None if pf is None else _ptr(pf),
+                                       0 if pf is None else len(pf), ctypes.byref(h)))
         self.h = h
         self.env_count = env_count
         self.max_cars = max_cars

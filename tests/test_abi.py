@@ -138,6 +138,10 @@ def test_pybind_module_mirrors_the_reference_binding(arena_mesh):
                  "step_with_device_commands", "reset_to_kickoff", "synchronize", "internal_state_layout",
                  "download_internal_state", "upload_internal_state"):
         assert hasattr(m.BatchSim, name), name
+    layout = m.ArenaLayout()
+    for name in ("meshes", "boost_pads", "goals", "kickoff_spawns", "respawn_spawns", "ball_spawn"):
+        assert hasattr(layout, name), name
+    assert layout.goals[1].point.y == layout.goals[1].point.y and len(layout.respawn_spawns[1]) == 4
     cfg = m.SimConfig()
     assert cfg.kickoff_settled == 0 and cfg.max_cars_per_env == 6
     v, i = arena_mesh
