@@ -295,11 +295,11 @@ RG_API int rg_batch_step_with_device_controls(rg_batch* b, const rg_car_controls
  * reset_scoreboard = 0: scores and tick kept and, with no seed, the match's next kickoff order; keep_boost_pads keeps
  * the pads); reset_scoreboard / reset_tick_count then clear the score / tick (only together with a reset, as in the
  * reference); new_round_bodies takes every body out of the broadphase as the game does after a goal. The host array
- * is borrowed for the call (the call synchronises the stream). kickoff_countdown_ticks != 0 (the game's countdown
- * spawn) is not built: such a command is refused (invalid_argument) and nothing is applied. */
+ * is borrowed for the call (the call synchronises the stream). kickoff_countdown_ticks != 0 is the game's countdown
+ * kickoff: cars appear at their spots a tick and a half later, driving stays off for that many ticks (0xFFFF: until
+ * the game's countdown timers end it, about 482 ticks), the ball starts awake at the game's drop height. */
 RG_API int rg_batch_apply_env_commands(rg_batch* b, const rg_env_command* host_commands, size_t count, void* stream);
-/* BatchSim::apply_env_commands_device (rocketgpu.h:1067): as above with a device array, asynchronous. A command with
- * kickoff_countdown_ticks != 0 leaves its env unchanged and the next rg_batch_synchronize reports invalid_argument. */
+/* BatchSim::apply_env_commands_device (rocketgpu.h:1067): as above with a device array, asynchronous. */
 RG_API int rg_batch_apply_env_commands_device(rg_batch* b, const rg_env_command* device_commands, size_t count,
                                               void* stream);
 /* BatchSim::step_with_device_commands (rocketgpu.h:1077; src/rocketgpu.cpp:2554-2575): as
@@ -340,8 +340,7 @@ RG_API int rg_batch_get_launch_config(const rg_batch* b, rg_launch_config* confi
 RG_API int rg_batch_phase_timing(rg_batch* b, int32_t enable);
 RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks);
 
-/* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch, and a device env
- * command that was refused (invalid_argument). */
+/* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
 
 /* Arenas on different geometries in one batch. The reference takes one geometry per BatchSim (ArenaLayout,

@@ -144,7 +144,7 @@ struct rg_batch {
     std::vector<StepGraph> graphs;
     uint64_t graph_clock = 0;
     DeviceArray<rg::EnvCommand> command_scratch;  // per arena: the host commands of rg_batch_apply_env_commands
-    DeviceArray<uint32_t> device_status;          // bit 0: a device command asked for something this build refuses
+    DeviceArray<uint32_t> device_status;          // reserved for device-side command errors (none today)
     DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
     DeviceArray<uint64_t> episode_seen;           // per car slot: latest_touch_tick at the previous episode check
     // Phase timing (rg_batch_phase_timing): events around the six kernels of every tick, seven per tick.
@@ -338,16 +338,6 @@ __device__ __forceinline__ rg::ArenaContactState arena_contact_state(const CarTi
     return cs;
 }
 
-// A command this build does not run (the game's countdown spawn): flag it for the host instead of resetting
-// differently from the reference; the arena is left as it was.
-__device__ __forceinline__ bool command_refused(const rg::EnvCommand& c, uint32_t* status) {
-    if (c.reset_to_kickoff && c.kickoff_countdown_ticks != 0) {
-        atomicOr(status, 1u);
-        return true;
-    }
-    return false;
-}
-
 // Env commands between steps, one thread per arena (reference LaunchApplyEnvCommands / apply_env_commands_host,
 // src/rocketgpu.cpp:2136-2218).
 __global__ void apply_commands_kernel(CarTickArgs a, const rg::EnvCommand* cmds, int n, rg::CarControls* controls,
@@ -355,7 +345,7 @@ __global__ void apply_commands_kernel(CarTickArgs a, const rg::EnvCommand* cmds,
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     const rg::EnvCommand c = cmds[e];
-    if (!rg::env_command_active(c) || command_refused(c, status)) return;
+    if (!rg::env_command_active(c)) return;
     rg::ArenaCars A = arena_cars(a, e, 0);
     rg::apply_env_command(c, e, a.base.envs[e], a.base.balls[e], arena_contact_state(a, e), A,
                           controls + static_cast<size_t>(e) * a.max_cars, a.pad_layout, a.base.tc);
@@ -370,14 +360,15 @@ __global__ void __launch_bounds__(256) arena_begin_kernel(CarTickArgs a, int t) 
     if (arena_idle(a, e)) return;
     if (a.commands) {
         const rg::EnvCommand c = a.commands[static_cast<size_t>(t) * static_cast<size_t>(a.command_stride) + e];
-        if (rg::env_command_active(c) && !command_refused(c, a.status))
+        if (rg::env_command_active(c))
             rg::apply_env_command(c, e, a.base.envs[e], a.base.balls[e], arena_contact_state(a, e),
                                   arena_cars(a, e, t), a.reset_controls + static_cast<size_t>(e) * a.max_cars,
                                   a.pad_layout, a.base.tc);
     }
     rg::BallState b = a.base.balls[e];
     rg::EnvState env = a.base.envs[e];
-    rg::arena_tick_begin(env, b, arena_cars(a, e, t), a.base.tc, a.pad_layout, a.snaps[e]);
+    rg::arena_tick_begin(env, b, arena_cars(a, e, t), a.base.tc, a.pad_layout, a.snaps[e],
+                         a.slots.remaining ? a.slots.seed[e] : a.base.tc.kickoff_seed, logical_env(a, e));
     a.base.balls[e] = b;
     a.base.envs[e] = env;
 }
@@ -1096,7 +1087,7 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         if (cfg->max_cars_per_env < 0 || cfg->max_cars_per_env > 6)
             throw std::invalid_argument("max_cars_per_env must be in [0, 6]");
         // Kickoff settling (the reference's MutatorConfig::kickoff_settled, src/rocketgpu.cpp:1538-1603: kickoffs
-        // that start from the state the game's countdown leaves) is not built: refuse it instead of resetting
+        // that start from a pre-recorded settle of the countdown) is not built: refuse it instead of resetting
         // differently from the reference.
         if (cfg->kickoff_settled != 0)
             throw std::invalid_argument("kickoff_settled = 1 is not supported by this build; set it to 0");
@@ -1455,9 +1446,6 @@ RG_API int rg_batch_apply_env_commands(rg_batch* b, const rg_env_command* host, 
         size_t active = 0;
         for (size_t i = 0; i < count; ++i) {
             const rg_env_command& c = host[i];
-            if (c.reset_to_kickoff && c.kickoff_countdown_ticks != 0)
-                throw std::invalid_argument("kickoff_countdown_ticks != 0 is not supported (the game's countdown spawn "
-                                            "is not built)");
             active += (c.reset_to_kickoff | c.reset_scoreboard | c.reset_tick_count | c.new_round_bodies) != 0;
         }
         if (active == 0) return;
@@ -1581,14 +1569,6 @@ RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
         if (!b) throw std::invalid_argument("null argument");
         DeviceGuard dg(b->device);
         check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
-        uint32_t status = 0;
-        check(cudaMemcpy(&status, b->device_status.ptr, sizeof(status), cudaMemcpyDeviceToHost), "device status");
-        if (status) {
-            check(cudaMemset(b->device_status.ptr, 0, sizeof(status)), "device status");
-            throw std::invalid_argument(
-                "a device env command asked for kickoff_countdown_ticks != 0 (the game's countdown spawn is not "
-                "built); those arenas were left unchanged");
-        }
     });
 }
 

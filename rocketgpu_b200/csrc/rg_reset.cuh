@@ -139,6 +139,14 @@ RG_HDI void place_car_at_kickoff_spawn(CarState& c, int team, SpawnPos spawn, fl
     reset_car_common(c, boost);
 }
 
+// reference PendKickoffSpawn (arena_ball.hpp:2769-2773): at a game-spawn kickoff the car waits demolished for a tick
+// and a half, then respawns at its kickoff spot
+RG_HDI void pend_kickoff_spawn(CarState& c, int spot, float tick_dt) {
+    c.is_demoed = 1;
+    c.demo_respawn_timer = 1.5f * tick_dt;
+    c.respawn_slot_override_plus1 = static_cast<uint8_t>(kKickoffSpawnOverridePlus1 + spot);
+}
+
 // reference PlaceCarAtWorldSpawn (arena_ball.hpp:2579-2585): a custom arena's spawn, pos.z the ground
 RG_HDI void place_car_at_world_spawn(CarState& c, V3 pos, float yaw, float z, float boost) {
     car_set_pos_bt(c, V3{pos.x, pos.y, pos.z + z} * kUuToBt);
@@ -147,8 +155,9 @@ RG_HDI void place_car_at_world_spawn(CarState& c, V3 pos, float yaw, float z, fl
     reset_car_common(c, boost);
 }
 
-// reference ResetBall(ball, Soccar, game_spawn = false, rules) (arena_ball.hpp:2775-2815)
-RG_HDI void reset_kickoff_ball(BallState& b, const ArenaRules* rules = nullptr) {
+// reference ResetBall(ball, Soccar, game_spawn, rules) (arena_ball.hpp:2775-2815): a game spawn (the countdown's
+// kickoff) puts the ball at the height the game drops it from, awake
+RG_HDI void reset_kickoff_ball(BallState& b, const ArenaRules* rules = nullptr, bool game_spawn = false) {
     b.pos_bt = V3{0.0f, 0.0f, 93.15f} * kUuToBt;
     b.pos = b.pos_bt * 50.0f;
     b.rot = Q4{1.0f, 0.0f, 0.0f, 0.0f};
@@ -174,10 +183,19 @@ RG_HDI void reset_kickoff_ball(BallState& b, const ArenaRules* rules = nullptr) 
     b.sleeping = 0;
     b.deactivation_time = 0.0f;
     b.constrained_2d = 0;
-    const V3 p = rules ? rules->ball_spawn : V3{0.0f, 0.0f, 92.75f};
-    b.pos_bt = V3{p.x, p.y, p.z} * kUuToBt;
-    b.pos = b.pos_bt * 50.0f;
-    b.sleeping = 1;
+    if (rules) {
+        const V3 p = rules->ball_spawn;
+        b.pos_bt = V3{p.x, p.y, game_spawn ? p.z + (100.487184524536f - 92.75f) : p.z} * kUuToBt;
+        b.pos = b.pos_bt * 50.0f;
+        b.sleeping = game_spawn ? 0 : 1;
+    } else if (game_spawn) {
+        b.pos_bt = V3{0.0f, 0.0f, 2.0097436904907227f};
+        b.pos = b.pos_bt * 50.0f;
+    } else {
+        b.pos_bt = V3{0.0f, 0.0f, 92.75f} * kUuToBt;
+        b.pos = b.pos_bt * 50.0f;
+        b.sleeping = 1;
+    }
 }
 
 // reference KickoffSpotPreferred / PreferKickoffSpotForShortTeam (arena_ball.hpp:2632-2653): a team with fewer cars
@@ -212,6 +230,7 @@ struct KickoffReset {
     uint8_t seed_mode = 0;        // 0: spot order from the seed (0: from the reset count); 2: as 0 with seed 0;
                                   // 3: no shuffle, a team's nth car takes kickoff spot n
     bool keep_pads = false;       // keep the pads and their timers
+    bool game_spawn = false;      // the countdown's kickoff: cars appear at their spots a tick and a half later
 };
 
 // The car slot visited k-th under `env`'s visit order (reference CarVisitSlot, rocketgpu.h:575-581).
@@ -301,7 +320,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
     for (int t = 0; t < 2; ++t)
         for (int i = 0; i < 5; ++i) order_bits[t] |= static_cast<uint32_t>(team_order[t][i]) << (3 * i);
 
-    reset_kickoff_ball(ball, rules);
+    reset_kickoff_ball(ball, rules, how.game_spawn);
     if (pads && !how.keep_pads) {
         for (int p = 0; p < L.count; ++p) {
             PadState& pad = pads[p];
@@ -338,6 +357,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
             const float yaw = nth < 5 ? rules->kickoff_yaw[t][spot] : rules->respawn_yaw[t][r];
             if (nth >= 5) pos = pos - V3{game_cosf(yaw), game_sinf(yaw), 0.0f} * step;
             place_car_at_world_spawn(cars[i], pos, yaw, cfgs[i].spawn_z, tc.boost_spawn_amount);
+            if (how.game_spawn && nth < 5) pend_kickoff_spawn(cars[i], spot, tc.tick_dt);
             continue;
         }
         SpawnPos spawn;
@@ -352,6 +372,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
             spawn = soccar_kickoff_spawn(spot);
         }
         place_car_at_kickoff_spawn(cars[i], team, spawn, cfgs[i].spawn_z, tc.boost_spawn_amount);
+        if (how.game_spawn && nth < 5) pend_kickoff_spawn(cars[i], spot, tc.tick_dt);
     }
 }
 

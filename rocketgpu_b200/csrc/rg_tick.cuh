@@ -1,10 +1,11 @@
-// One 120 Hz tick of one arena (host+device). Ball-only arenas in this build: the ball's pre-tick network
-// quantisation, speed caps and drag, Bullet activation / sleeping, the world step (gravity, contacts with the arena
-// mesh, integration) and the tail (ball finish, goal test, render-frame timers, tick counter).
+// One 120 Hz tick of one arena (host+device): env commands and the tick-start env state (the game's car order,
+// respawn-spot picks), each car's tick start and vehicle update, the world step (ball and cars against the arena mesh
+// and each other, the unified velocity and split solves, integration), each car's post-tick and the tail (pads, the
+// driving countdown, ball hits, goals, render-frame timers, tick counter).
 //
 // Phase order and arithmetic follow the reference's per-env tick, StepEnvGeneric
-// (include/rocketgpu/detail/step/env_step.hpp:7048-7180), with the ball-only branches of WorldStepSoccar
-// (env_step.hpp:4622-5623) and StepEnvTail (env_step.hpp:6968-7045).
+// (include/rocketgpu/detail/step/env_step.hpp:7048-7180), with WorldStepSoccar (env_step.hpp:4622-5623) and
+// StepEnvTail (env_step.hpp:6968-7045).
 #pragma once
 
 #include "rg_ball_car.cuh"
@@ -355,6 +356,166 @@ RG_HDI SpawnPos soccar_respawn_spawn(int i) {
         default: return SpawnPos{2688.0f, -4608.0f, kPiF * 0.5f};
     }
 }
+// The ground point and yaw of a team's respawn spot, moved 192 uu in one of eight directions around the spot's facing
+// when dir >= 0 (reference RespawnPlace, arena_ball.hpp:3098-3122).
+RG_HDI void respawn_place(int team, int spot, int dir, const ArenaRules* rules, V3& ground, float& yaw) {
+    const bool blue = team == 0;
+    float fx = 0.0f, fy = blue ? 1.0f : -1.0f;
+    if (rules) {
+        const int t = blue ? 0 : 1;
+        ground = rules->respawn_pos[t][spot & 3];
+        yaw = rules->respawn_yaw[t][spot & 3];
+        const Q4 q = quat_from_yaw(wrap_angle(yaw));
+        fx = q.w * q.w - q.z * q.z;
+        fy = 2.0f * q.w * q.z;
+    } else {
+        const SpawnPos s = soccar_respawn_spawn(spot & 3);
+        ground = V3{s.x, blue ? s.y : -s.y, 0.0f};
+        yaw = s.yaw + (blue ? 0.0f : kPiF);
+    }
+    if (dir >= 0) {
+        constexpr float k = 0.70710677f;
+        const int d = dir & 7;
+        const float ux = d == 0 ? 1.0f : (d == 1 || d == 7) ? k : (d == 2 || d == 6) ? 0.0f : (d == 3 || d == 5) ? -k : -1.0f;
+        const float uy = (d == 0 || d == 4) ? 0.0f : (d == 1 || d == 3) ? k : d == 2 ? 1.0f : d == 6 ? -1.0f : -k;
+        ground.x += 192.0f * (fx * ux - fy * uy);
+        ground.y += 192.0f * (fx * uy + fy * ux);
+    }
+}
+
+// Each car body's stored mesh bounds by CarConfig::body, unknown bodies reading the Octane's (reference
+// CarBodyMeshBounds, env_step.hpp:6546-6553).
+namespace body_bounds_host {
+#define RG_BODY_BOUNDS_TABLE(name, n) static const float name[n][6]
+#include "rg_body_bounds.inc"
+#undef RG_BODY_BOUNDS_TABLE
+}  // namespace body_bounds_host
+#if defined(__CUDACC__)
+namespace body_bounds_dev {
+#define RG_BODY_BOUNDS_TABLE(name, n) __device__ static const float name[n][6]
+#include "rg_body_bounds.inc"
+#undef RG_BODY_BOUNDS_TABLE
+}  // namespace body_bounds_dev
+#endif
+constexpr int kBodyCount = static_cast<int>(sizeof(body_bounds_host::kBodyMeshBounds) / sizeof(float[6]));
+constexpr int kBodyOctane = 147;
+RG_HDI const float* body_mesh_bounds(int body) {
+    const int b = body >= 0 && body < kBodyCount ? body : kBodyOctane;
+#if defined(__CUDA_ARCH__)
+    return body_bounds_dev::kBodyMeshBounds[b];
+#else
+    return body_bounds_host::kBodyMeshBounds[b];
+#endif
+}
+
+// Whether a spawn point lies within 48 uu of an axis-aligned box (reference SpawnSpotNearBox, env_step.hpp:6538-6543).
+RG_HDI bool spawn_spot_near_box(V3 spot, V3 center, V3 half) {
+    const float dx = fmax_(fabs_(spot.x - center.x) - half.x, 0.0f);
+    const float dy = fmax_(fabs_(spot.y - center.y) - half.y, 0.0f);
+    const float dz = fmax_(fabs_(spot.z - center.z) - half.z, 0.0f);
+    return dx * dx + dy * dy + dz * dz <= 48.0f * 48.0f;
+}
+// ... of a car: a box at its origin, or its body's mesh bounds turned into a world-axis box (reference
+// SpawnSpotNearCar, env_step.hpp:6556-6564).
+RG_HDI bool spawn_spot_near_car(V3 spot, V3 pos, V3 fwd, V3 right, V3 up, const float* bounds) {
+    if (spawn_spot_near_box(spot, pos, V3{48.0f, 48.0f, 32.0f})) return true;
+    const V3 center = pos + fwd * bounds[0] + right * bounds[1] + up * bounds[2];
+    return spawn_spot_near_box(spot, center,
+                               V3{fabs_(fwd.x) * bounds[3] + fabs_(right.x) * bounds[4] + fabs_(up.x) * bounds[5],
+                                  fabs_(fwd.y) * bounds[3] + fabs_(right.y) * bounds[4] + fabs_(up.y) * bounds[5],
+                                  fabs_(fwd.z) * bounds[3] + fabs_(right.z) * bounds[4] + fabs_(up.z) * bounds[5]});
+}
+// Whether a respawn ground point is taken: near another car where it is now, or (a demolished car) where it comes
+// back this tick or, for an earlier slot also due, where its spot was already picked; or near the ball (reference
+// RespawnPlaceTaken, env_step.hpp:6566-6613).
+RG_HDI bool respawn_place_taken(V3 ground, int self, const ArenaCars& A, uint32_t demoed, uint32_t due,
+                                const TickConfig& tc, V3 ball_pos) {
+    const V3 spot{ground.x, ground.y, ground.z + 83.0f};
+    for (int j = 0; j < A.count && j < 32; ++j) {
+        if (j == self) continue;
+        const CarState& o = A.cars[j];
+        V3 pos, fwd, right, up;
+        if (((demoed >> j) & 1u) == 0u) {
+            car_basis(o, fwd, right, up);
+            pos = o.pos_bt * 50.0f;
+        } else {
+            const bool back_now = !(fmax_(0.0f, o.demo_respawn_timer - tc.tick_dt) > 0.0f);
+            if (!back_now && (j > self || ((due >> j) & 1u) == 0u)) continue;
+            const int code = o.respawn_slot_override_plus1;
+            int s = -1, d = -1;
+            if (code >= kRespawnOffsetOverridePlus1 && code < kRespawnOffsetOverridePlus1 + 32) {
+                s = ((code - kRespawnOffsetOverridePlus1) >> 3) & 3;
+                d = (code - kRespawnOffsetOverridePlus1) & 7;
+            } else if (code != 0) {
+                if (code >= kKickoffSpawnOverridePlus1) continue;
+                s = code - 1;
+            } else {
+                continue;
+            }
+            float yaw;
+            respawn_place(A.teams[j], s, d, tc.rules, pos, yaw);
+            pos.z += A.cfgs[j].spawn_z;
+            const Q4 q = quat_from_yaw(wrap_angle(yaw));
+            fwd = V3{q.w * q.w - q.z * q.z, 2.0f * q.w * q.z, 0.0f};
+            right = V3{-fwd.y, fwd.x, 0.0f};
+            up = V3{0.0f, 0.0f, 1.0f};
+        }
+        if (spawn_spot_near_car(spot, pos, fwd, right, up, body_mesh_bounds(A.cfgs[j].body))) return true;
+    }
+    const float r = tc.ball_radius;
+    return spawn_spot_near_box(spot, ball_pos, V3{r, r, r}) ||
+           spawn_spot_near_box(spot, ball_pos, V3{34.0f, 34.0f, 78.0f});
+}
+// The respawn spots of the arena's demolished cars that come back within two ticks, picked one tick ahead: the
+// arena's spot order from the draw's start, the first free spot, else its eight 192 uu neighbours one ring of spots at
+// a time, else the drawn spot; stored as the car's respawn override (reference PickRespawnSpotsForEnv,
+// env_step.hpp:6615-6650, called from StepEnvPreTickEnvState, env_step.hpp:6664-6693).
+RG_HDI void pick_respawn_spots(const ArenaCars& A, const BallState& b, const EnvState& env, const TickConfig& tc,
+                               uint64_t seed, int env_idx) {
+    const int count = A.count;
+    uint32_t demoed = 0;
+    if (env.car_visit_order_mode == 3 && count <= 8) {
+        demoed = ~static_cast<uint32_t>(env.car_visit_present_mask) & ((1u << count) - 1u);
+    } else {
+        for (int i = 0; i < count && i < 32; ++i) demoed |= static_cast<uint32_t>(A.cars[i].is_demoed != 0) << i;
+    }
+    if (demoed == 0) return;
+    uint32_t due = 0;
+    for (int i = 0; i < count && i < 32; ++i) {
+        if (((demoed >> i) & 1u) == 0u) continue;
+        const float left = fmax_(0.0f, A.cars[i].demo_respawn_timer - tc.tick_dt);
+        if (!(fmax_(0.0f, left - tc.tick_dt) > 0.0f)) due |= 1u << i;
+    }
+    if (due == 0) return;
+    const V3 ball_pos = b.pos_bt * 50.0f;
+    const uint32_t order = env.respawn_match_order != 0 ? env.respawn_match_order : build_respawn_order(seed, env_idx);
+    for (int i = 0; i < count && i < 32; ++i) {
+        if (((due >> i) & 1u) == 0u) continue;
+        CarState& car = A.cars[i];
+        if (car.respawn_slot_override_plus1 != 0) continue;
+        const int team = A.teams[i];
+        const int start = respawn_start_index(seed, env_idx, static_cast<uint64_t>(env.tick),
+                                              static_cast<uint32_t>(A.car_base + i + 1));
+        const int flip = team == 0 ? 0 : 2;
+        int spot = -1, dir = -1;
+        for (int k = 0; k < 36 && spot < 0; ++k) {
+            const int walk = k < 4 ? k : (k - 4) >> 3;
+            const int d = k < 4 ? -1 : (k - 4) & 7;
+            const int s = static_cast<int>((order >> (2 * ((start + walk) & 3))) & 3u) ^ flip;
+            V3 ground;
+            float yaw;
+            respawn_place(team, s, d, tc.rules, ground, yaw);
+            if (!respawn_place_taken(ground, i, A, demoed, due, tc, ball_pos)) {
+                spot = s;
+                dir = d;
+            }
+        }
+        if (spot < 0) spot = static_cast<int>((order >> (2 * (start & 3))) & 3u) ^ flip;
+        car.respawn_slot_override_plus1 =
+            static_cast<uint8_t>(dir < 0 ? spot + 1 : kRespawnOffsetOverridePlus1 + 8 * spot + dir);
+    }
+}
+
 RG_HDI void respawn_car(CarState& c, const CarConfig& cfg, const TickConfig& tc, const RespawnCtx& rc) {
     const int team = rc.team;
     int slot = -1, offset_dir = -1;
@@ -382,20 +543,9 @@ RG_HDI void respawn_car(CarState& c, const CarConfig& cfg, const TickConfig& tc,
             c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
             return;
         }
-        const int rs = (slot % 4) & 3;
-        V3 ground = R.respawn_pos[t][rs];
-        const float yaw = R.respawn_yaw[t][rs];
-        if (offset_dir >= 0) {
-            const Q4 q = quat_from_yaw(wrap_angle(yaw));
-            const float fx = q.w * q.w - q.z * q.z;
-            const float fy = 2.0f * q.w * q.z;
-            constexpr float k = 0.70710677f;
-            const int d = offset_dir & 7;
-            const float ux = d == 0 ? 1.0f : (d == 1 || d == 7) ? k : (d == 2 || d == 6) ? 0.0f : (d == 3 || d == 5) ? -k : -1.0f;
-            const float uy = (d == 0 || d == 4) ? 0.0f : (d == 1 || d == 3) ? k : d == 2 ? 1.0f : d == 6 ? -1.0f : -k;
-            ground.x += 192.0f * (fx * ux - fy * uy);
-            ground.y += 192.0f * (fx * uy + fy * ux);
-        }
+        V3 ground;
+        float yaw;
+        respawn_place(team, slot % 4, offset_dir, tc.rules, ground, yaw);
         place_car_at_world_spawn(c, ground, yaw, cfg.spawn_z, tc.boost_spawn_amount);
         c.vel_impulse_cache = V3{0.0f, 0.0f, 0.0f};
         c.is_on_ground = 0;
@@ -411,17 +561,11 @@ RG_HDI void respawn_car(CarState& c, const CarConfig& cfg, const TickConfig& tc,
     }
     SpawnPos spawn = soccar_respawn_spawn(slot % 4);
     if (offset_dir >= 0) {
-        const bool blue = team == 0;
-        const float fx = 0.0f, fy = blue ? 1.0f : -1.0f;
-        float gx = spawn.x, gy = blue ? spawn.y : -spawn.y;
-        constexpr float k = 0.70710677f;
-        const int d = offset_dir & 7;
-        const float ux = d == 0 ? 1.0f : (d == 1 || d == 7) ? k : (d == 2 || d == 6) ? 0.0f : (d == 3 || d == 5) ? -k : -1.0f;
-        const float uy = (d == 0 || d == 4) ? 0.0f : (d == 1 || d == 3) ? k : d == 2 ? 1.0f : d == 6 ? -1.0f : -k;
-        gx += 192.0f * (fx * ux - fy * uy);
-        gy += 192.0f * (fx * uy + fy * ux);
-        spawn.x = gx;
-        spawn.y = blue ? gy : -gy;
+        V3 ground;
+        float yaw;
+        respawn_place(team, slot % 4, offset_dir, nullptr, ground, yaw);
+        spawn.x = ground.x;
+        spawn.y = team == 0 ? ground.y : -ground.y;
     }
     // reference PlaceCarAtRespawnSpawn (arena_ball.hpp:2562-2577): x is not mirrored for orange
     const float y = team == 0 ? spawn.y : -spawn.y;
@@ -1473,10 +1617,12 @@ struct ArenaTickSnap {
     V3 ball_start_vel, ball_vel_bt;
 };
 
+// respawn_seed and env_idx are the respawn draw's: the batch's last kickoff seed and the arena's logical index.
 RG_HDI void arena_tick_begin(EnvState& env, BallState& b, const ArenaCars& A, const TickConfig& c,
-                             const PadLayout& pads_layout, ArenaTickSnap& as) {
+                             const PadLayout& pads_layout, ArenaTickSnap& as, uint64_t respawn_seed, int env_idx) {
     const int count = A.count;
     update_game_visit_order(env, A.cars, count);
+    pick_respawn_spots(A, b, env, c, respawn_seed, env_idx);
     env.goal_scored_this_tick = 0;
     ball_tick_start_quantize(b, c);
     as.ball_start_vel = b.vel;
@@ -1603,6 +1749,9 @@ RG_HDI void arena_tick_tail(EnvState& env, BallState& b, const ArenaCars& A, con
 
 // ---- env commands ------------------------------------------------------------------------------------------------
 // One arena's command (byte-identical to rg_env_command / the reference's EnvCommand, rocketgpu.h:683-706).
+constexpr uint16_t kKickoffCountdownTicks = 480;         // reference rocketgpu.h:632: driving off for 4 s
+constexpr uint16_t kKickoffCountdownGameTimers = 0xFFFF;  // reference rocketgpu.h:635: until the game timers end it
+
 struct EnvCommand {
     uint8_t reset_to_kickoff, reset_scoreboard, reset_tick_count, kickoff_seed_mode, new_round_bodies, keep_boost_pads;
     uint16_t kickoff_countdown_ticks;
@@ -1641,7 +1790,9 @@ RG_HDI void clear_retained_car_contacts(const ArenaContactState& s, int max_cars
 //   * reset_to_kickoff: the arena's kickoff (the match's next kickoff when the scoreboard is kept and no seed is
 //     given), every retained contact cleared, then the scoreboard / tick counter / countdown fields of the env.
 // A command without reset_to_kickoff changes no env field (the reference applies the env fields only with a reset).
-// kickoff_countdown_ticks must be 0 (the game's countdown spawn is not built; the batch refuses others).
+// kickoff_countdown_ticks != 0 makes it the game's countdown kickoff (cars held and placed a tick and a half later,
+// driving off for that many ticks or, at 0xFFFF, until the countdown timers end it, the ball dropped from the game's
+// height).
 RG_HDI void apply_env_command(const EnvCommand& cmd, int env_idx, EnvState& env, BallState& ball,
                               const ArenaContactState& cs, const ArenaCars& A, CarControls* controls,
                               const PadLayout& L, const TickConfig& tc) {
@@ -1661,11 +1812,14 @@ RG_HDI void apply_env_command(const EnvCommand& cmd, int env_idx, EnvState& env,
     how.preserve_score = cmd.reset_scoreboard == 0;
     how.seed_mode = cmd.kickoff_seed_mode;
     how.keep_pads = cmd.keep_boost_pads != 0;
+    how.game_spawn = cmd.kickoff_countdown_ticks != 0;
     reset_env_to_kickoff(env_idx, cmd.kickoff_seed, env, ball, *cs.ball_world, A.cars, A.cfgs, controls, A.pads, L,
                          A.teams, count, A.max_cars, tc, how);
     clear_retained_car_contacts(cs, A.max_cars);
-    for (int k = 0; k < count; ++k) A.cars[car_visit_slot(env, k, count)].driving_disabled = 0;
-    ball.constrained_2d = 0;
+    // the countdown: driving off for its ticks (or until the game timers end it), the ball held in its plane
+    // (reference ApplyEnvCommand, env_step.hpp:5747-5752)
+    for (int k = 0; k < count; ++k) A.cars[car_visit_slot(env, k, count)].driving_disabled = cmd.kickoff_countdown_ticks;
+    ball.constrained_2d = cmd.kickoff_countdown_ticks;
     if (cmd.reset_scoreboard) {
         env.blue_score = 0;
         env.orange_score = 0;
@@ -1673,7 +1827,7 @@ RG_HDI void apply_env_command(const EnvCommand& cmd, int env_idx, EnvState& env,
     }
     if (cmd.reset_tick_count) env.tick = 0;
     env.goal_scored_this_tick = 0;
-    env.countdown_phase = 0;
+    env.countdown_phase = cmd.kickoff_countdown_ticks == kKickoffCountdownGameTimers ? 1 : 0;
     env.countdown_fires = 0;
     env.countdown_count = 0.0f;
 }

@@ -161,3 +161,48 @@ def test_six_hitbox_presets(oracle_available, arena_mesh):
             gpu.synchronize()
             d = _compare(orc, gpu, counts)
             assert d is None, f"launch {launch} tick {t}: {d}"
+
+
+OFF_RESPAWN_OVERRIDE = 138  # CarState.respawn_slot_override_plus1
+
+
+def test_respawn_spot_picks_1600_ticks(oracle_available, arena_mesh):
+    """Long chase with the six hitbox presets, so demolished cars come back many times: each one's respawn spot is
+    picked a tick ahead, walking the arena's spot order and the eight moved spots around each, clear of the other cars
+    (where they are, or where they come back, by their bodies' mesh bounds) and of the ball; 1,600 ticks compared after
+    every tick, the picks counted."""
+    import torch
+    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
+    n, k, launches = 96, 8, 200
+    counts, teams = _arenas(n, 23)
+    rng = np.random.default_rng(30)
+    cfgs = np.stack([oracle_ref.car_preset(int(p)) for p in rng.integers(0, 6, n * MC)])
+    v, i = arena_mesh
+    orc = oracle_ref.OracleSim(n, MC, v, i, kickoff_settled=False)
+    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC, kickoff_settled=0), v, i)
+    for sim in (orc, gpu):
+        sim.set_env_car_count(counts)
+        sim.set_teams(teams)
+        sim.set_car_configs(cfgs)
+        sim.reset_to_kickoff(23)
+    gpu.synchronize()
+    act = np.concatenate([np.arange(e * MC, e * MC + counts[e]) for e in range(n)])
+    crng = np.random.default_rng(523)
+    prev = np.zeros(len(act), np.uint8)
+    picks = moved = 0
+    for launch in range(launches):
+        ctrl = scenarios.chase_ball_controls(orc.cars(), orc.balls(), MC, crng, p_jump=0.03)
+        dev = torch.from_numpy(ctrl).cuda()
+        for t in range(k):
+            orc.step_with_controls(ctrl, 1, 0)
+            gpu.step_with_device_controls(dev.data_ptr(), 1, 0)
+            gpu.synchronize()
+            d = _compare(orc, gpu, counts)
+            assert d is None, f"launch {launch} tick {t}: {d} ({picks} respawn picks so far)"
+            cur = orc.cars()[act, OFF_RESPAWN_OVERRIDE]
+            new = (prev == 0) & (cur != 0)
+            picks += int(new.sum())
+            moved += int((new & (cur >= 128)).sum())
+            prev = cur.copy()
+    assert picks > 10, picks
+    print(f"{picks} respawn spot picks, {moved} of them moved off a taken spot")

@@ -151,21 +151,43 @@ def test_goal_and_no_touch_resets_2000_ticks(oracle_available, arena_mesh):
     print(f"{resets} episode resets over {steps * k} ticks of {n} arenas")
 
 
-def test_countdown_commands_are_refused(arena_mesh):
+def test_countdown_kickoffs(oracle_available, arena_mesh):
+    """Countdown kickoffs (kickoff_countdown_ticks: 480 ticks, and 0xFFFF, until the game's countdown timers end it):
+    cars wait a tick and a half then appear at their spots, driving stays off, the ball drops from the game's height;
+    between steps (host and device arrays) and inside launches, through the end of the countdown."""
     import torch
-    from rocketgpu_b200.batch_sim import BatchSim, SimConfig
-    v, i = arena_mesh
-    gpu = BatchSim(SimConfig(env_count=4, max_cars_per_env=2), v, i)
-    gpu.set_env_car_count([2, 2, 2, 2])
-    cmds = np.zeros((4, 16), np.uint8)
-    cmds[1, 0] = 1
-    cmds[1, 6] = 1  # kickoff_countdown_ticks = 1
-    with pytest.raises(ValueError, match="countdown"):
-        gpu.apply_env_commands(cmds)
-    before = gpu.download_car_states()
-    dev = torch.from_numpy(cmds).cuda()
-    gpu.apply_env_commands_device(dev.data_ptr(), 4)
-    with pytest.raises(ValueError, match="countdown"):
+    n, k = 48, 8
+    counts, teams = _arenas(n, 91)
+    orc, gpu = _pair(n, arena_mesh, counts, teams, 91)
+    rng = np.random.default_rng(91)
+    crng = np.random.default_rng(92)
+    for rnd in range(3):
+        cmds = np.zeros((n, 16), np.uint8)
+        sel = rng.random(n) < 0.6
+        cmds[sel, 0] = 1
+        cmds[sel, 1] = rng.random(sel.sum()) < 0.5
+        ticks = np.where(rng.random(n) < 0.5, 480, 0xFFFF).astype(np.uint16)
+        cmds[:, 6:8] = ticks.view(np.uint8).reshape(n, 2)
+        cmds[:, 3] = rng.choice([0, 3], n)
+        orc.apply_env_commands(cmds)
+        if rnd == 1:
+            dev = torch.from_numpy(cmds).cuda()
+            gpu.apply_env_commands_device(dev.data_ptr(), n)
+        else:
+            gpu.apply_env_commands(cmds)
         gpu.synchronize()
-    assert np.array_equal(before, gpu.download_car_states())
-    gpu.synchronize()  # the flag is cleared once reported
+        d = _compare(orc, gpu, counts)
+        assert d is None, f"round {rnd} after commands: {d}"
+        for step in range(70):  # 560 ticks: past the countdown's end
+            ctrl = scenarios.chase_ball_controls(orc.cars(), orc.balls(), MC, crng, p_jump=0.05)
+            cm = np.zeros((k, n, 16), np.uint8)
+            if rnd == 2 and step == 3:  # a countdown kickoff inside a launch
+                cm[5, :, 0] = 1
+                cm[5, :, 6:8] = np.full(n, 480, np.uint16).view(np.uint8).reshape(n, 2)
+            dev_ctrl = torch.from_numpy(ctrl).cuda()
+            dev_cmds = torch.from_numpy(cm.reshape(-1, 16).copy()).cuda()
+            orc.step_with_commands(ctrl, 0, cm.reshape(-1, 16), n, k)
+            gpu.step_with_device_commands(dev_ctrl.data_ptr(), 0, dev_cmds.data_ptr(), n, k)
+            gpu.synchronize()
+            d = _compare(orc, gpu, counts)
+            assert d is None, f"round {rnd} step {step}: {d}"
