@@ -333,7 +333,7 @@ def run_ours(args, world, rank, local):
 
     def make_sim():
         if mixed:
-            sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=MAX_CARS), v, i, device=local)
+            sim = BatchSim(SimConfig(kickoff_settled=0, env_count=ENVS, max_cars_per_env=MAX_CARS), v, i, device=local)
             sim.set_env_car_count(w.counts)
             sim.set_teams(w.teams)
             sim.set_car_configs(w.car_configs(presets))
@@ -343,7 +343,7 @@ def run_ours(args, world, rank, local):
                                                 ctypes.c_void_p(cmds.data_ptr()), s_handle))
             return sim, cmds
         from tests import scenarios
-        sim = BatchSim(SimConfig(env_count=ENVS, max_cars_per_env=2), v, i, device=local)
+        sim = BatchSim(SimConfig(kickoff_settled=0, env_count=ENVS, max_cars_per_env=2), v, i, device=local)
         sim.set_env_car_count(np.zeros(ENVS, np.int32))
         default_ball = np.zeros(BALL_BYTES, np.uint8)
         lib.rg_default_ball_state(default_ball.ctypes.data)

@@ -180,8 +180,11 @@ typedef struct rg_sim_config {
     float gravity_z, ball_radius, ball_mass, car_mass, ball_drag, ball_friction, ball_restitution, ball_max_speed,
         ball_max_ang_speed, car_max_speed, car_max_ang_speed, arena_friction, arena_restitution,
         goal_base_threshold_y;
-    /* Must be 0: kickoff settling (reference MutatorConfig::kickoff_settled, default 1 there) is not built, so
-     * rg_sim_config_default sets 0 and rg_batch_create refuses 1 (status 2). */
+    /* reference MutatorConfig::kickoff_settled (rocketgpu.h:831, default 1 there and here). 1: a kickoff without a
+     * countdown puts each car into the state the game's countdown leaves at its spot (and the ball into the state it
+     * leaves), recorded once per (car config, team) by stepping a countdown kickoff (src/rocketgpu.cpp:1439-1612);
+     * recorded at create and before a reset after set_car_configs / set_teams / set_env_car_count. A batch with 1
+     * takes no further geometry (rg_batch_add_mesh) and the server takes 0. */
     uint8_t kickoff_settled;
     uint8_t reserved[7];
 } rg_sim_config;
@@ -275,8 +278,8 @@ RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, vo
 /* BatchSim::reset_to_kickoff (rocketgpu.h:1070; src/rocketgpu.cpp:2085-2132, ResetEnvToKickoff arena_ball.hpp:
  * 3054-3085): every arena to kickoff, the spot order drawn from `seed` (0: from the arena's reset count). Car
  * contact state and the ball's manifolds are cleared; wheel records are kept, as the reference keeps them.
- * rg_batch_create ends with reset_to_kickoff(0). The reset is the reference's with kickoff_settled = 0 (the only
- * value rg_batch_create accepts). */
+ * rg_batch_create ends with reset_to_kickoff(0). With kickoff_settled = 1 the cars and the ball take their settled
+ * states (rg_sim_config). */
 RG_API int rg_batch_reset_to_kickoff(rg_batch* b, uint64_t seed, void* stream);
 /* BatchSim::upload_controls (rocketgpu.h:1032): the controls rg_batch_step holds for every tick. */
 RG_API int rg_batch_upload_controls(rg_batch* b, const rg_car_controls* host, size_t count, void* stream);

@@ -147,6 +147,27 @@ struct rg_batch {
     DeviceArray<uint32_t> device_status;          // reserved for device-side command errors (none today)
     DeviceArray<int64_t> episode_touch;           // per arena: the episode's latest ball touch (env ticks)
     DeviceArray<uint64_t> episode_seen;           // per car slot: latest_touch_tick at the previous episode check
+    // Kickoff settling (cfg.kickoff_settled = 1): the create-time layout, kept to build the batch that records the
+    // countdown; the (car config, team) entries recorded so far with their rows (settled_spawns per entry) and the
+    // ball; the device copies b->tc.settled_* point at. New configs or teams record their entries before the next
+    // reset (reference ensure_kickoff_settled, src/rocketgpu.cpp:1439-1500).
+    std::vector<float> layout_vertices;
+    std::vector<int32_t> layout_indices;
+    bool layout_has_rules = false;
+    rg_arena_rules layout_rules{};
+    bool layout_has_pads = false;
+    std::vector<rg_boost_pad_config> layout_pads;
+    struct SettleEntry {
+        rg::CarConfig config;
+        uint8_t team;
+    };
+    std::vector<SettleEntry> settle_entries;
+    std::vector<rg::KickoffSettledRow> settle_rows_host;
+    std::vector<rg::BallState> settle_ball_host;
+    bool settle_dirty = true;
+    DeviceArray<rg::KickoffSettledRow> settle_rows;
+    DeviceArray<int32_t> settle_entry;
+    DeviceArray<rg::BallState> settle_ball;
     // Phase timing (rg_batch_phase_timing): events around the six kernels of every tick, seven per tick.
     bool timing = false;
     std::vector<cudaEvent_t> events;
@@ -321,6 +342,7 @@ __device__ __forceinline__ rg::ArenaCars arena_cars(const CarTickArgs& a, int e,
                             : nullptr;
     A.teams = a.teams + car_base;
     A.pairs = a.pair_slots ? a.pairs + static_cast<size_t>(e) * a.pair_slots : nullptr;
+    A.settled_entry = a.base.tc.settled_entry ? a.base.tc.settled_entry + car_base : nullptr;
     A.count = a.base.env_car_count[e];
     A.max_cars = a.max_cars;
     A.car_base = logical_env(a, e) * a.max_cars;  // car ids are car_base + slot + 1
@@ -651,9 +673,10 @@ __global__ void reset_kickoff_kernel(CarTickArgs a, const uint8_t* teams, rg::Ca
     }
     for (int k = 0; k < a.pair_slots; ++k) a.pairs[static_cast<size_t>(e) * a.pair_slots + k].count = 0;
     rg::reset_env_to_kickoff(j, seed, a.base.envs[e], a.base.balls[e], a.base.ball_world[e], a.cars + car_base,
-                             a.car_cfgs + car_base, controls + car_base,
+                             a.wheels + car_base, a.car_cfgs + car_base, controls + car_base,
                              a.pads ? a.pads + static_cast<size_t>(e) * a.pad_layout.count : nullptr, a.pad_layout,
-                             teams + car_base, a.base.env_car_count[e], a.max_cars, a.base.tc);
+                             teams + car_base, a.base.env_car_count[e], a.max_cars, a.base.tc,
+                             a.base.tc.settled_entry ? a.base.tc.settled_entry + car_base : nullptr);
 }
 
 // Episode resets for training loops (no counterpart in BatchSim; the reference's benchmark makes these decisions on
@@ -702,6 +725,132 @@ __global__ void episode_commands_kernel(const rg::EnvState* envs, const rg::CarS
     }
     touch[e] = last;
     out[e] = c;
+}
+
+void call_ok(int status, const char* what) {
+    if (status != 0) throw std::runtime_error(std::string("kickoff_settled: ") + what + ": " + rg_last_error());
+}
+
+// Records the settled kickoff of the entries first[] name (car slots whose config and team are new): one arena per
+// entry, `spawns` cars of that config and team, the game's countdown kickoff with the spots in order, stepped through
+// the countdown (480 ticks, then tick by tick until every arena's countdown has ended); car k's state and wheel record
+// become the entry's row for spot k, and the first recording's ball the settled ball (reference
+// record_kickoff_settled, src/rocketgpu.cpp:1538-1612).
+void record_kickoff_settled(rg_batch* b, const std::vector<size_t>& first, const std::vector<rg::CarConfig>& configs,
+                            const std::vector<uint8_t>& teams, int spawns) {
+    const size_t envs = first.size();
+    rg_sim_config rc = b->cfg;
+    rc.env_count = static_cast<int32_t>(envs);
+    rc.max_cars_per_env = spawns;
+    rc.kickoff_settled = 0;
+    rg_arena_layout L{};
+    L.vertices_uu = b->layout_vertices.data();
+    L.vertex_count = static_cast<int64_t>(b->layout_vertices.size() / 3);
+    L.indices = b->layout_indices.data();
+    L.index_count = static_cast<int64_t>(b->layout_indices.size());
+    L.rules = b->layout_has_rules ? &b->layout_rules : nullptr;
+    L.boost_pads = b->layout_has_pads ? b->layout_pads.data() : nullptr;
+    L.boost_pad_count = b->layout_has_pads ? static_cast<int32_t>(b->layout_pads.size()) : 0;
+    rg_batch* created = nullptr;
+    call_ok(rg_batch_create(&rc, &L, b->device, &created), "create");
+    std::unique_ptr<rg_batch, void (*)(rg_batch*)> run(created, rg_batch_destroy);
+    const size_t m = envs * static_cast<size_t>(spawns);
+    std::vector<int32_t> counts(envs, spawns);
+    std::vector<rg_car_config> run_cfgs(m);
+    std::vector<uint8_t> run_teams(m);
+    for (size_t i = 0; i < m; ++i) {
+        memcpy(&run_cfgs[i], &configs[first[i / spawns]], sizeof(rg_car_config));
+        run_teams[i] = teams[first[i / spawns]];
+    }
+    call_ok(rg_batch_set_env_car_count(run.get(), counts.data(), envs, nullptr), "car counts");
+    call_ok(rg_batch_set_teams(run.get(), run_teams.data(), m, nullptr), "teams");
+    call_ok(rg_batch_set_car_configs(run.get(), run_cfgs.data(), m, nullptr), "car configs");
+    rg_env_command cmd{};
+    cmd.reset_to_kickoff = 1;
+    cmd.reset_scoreboard = 1;
+    cmd.kickoff_seed_mode = 3;
+    cmd.kickoff_countdown_ticks = rg::kKickoffCountdownGameTimers;
+    std::vector<rg_env_command> cmds(envs, cmd);
+    call_ok(rg_batch_apply_env_commands(run.get(), cmds.data(), envs, nullptr), "countdown kickoff");
+    call_ok(rg_batch_step(run.get(), rg::kKickoffCountdownTicks, nullptr), "countdown");
+    std::vector<rg_env_state> env_out(envs);
+    for (int k = 0;; ++k) {
+        call_ok(rg_batch_download_env_states(run.get(), env_out.data(), envs, nullptr), "env states");
+        bool ended = true;
+        for (const rg_env_state& e : env_out) ended = ended && e.countdown_phase == 0;
+        if (ended) break;
+        if (k == 16) throw std::runtime_error("kickoff_settled: the countdown did not end");
+        call_ok(rg_batch_step(run.get(), 1, nullptr), "countdown");
+    }
+    std::vector<rg::CarState> cars(m);
+    std::vector<rg::WheelRuntime> wheels(m);
+    rg::BallState ball;
+    check(cudaMemcpy(cars.data(), run->cars.ptr, m * sizeof(rg::CarState), cudaMemcpyDeviceToHost), "settled cars");
+    check(cudaMemcpy(wheels.data(), run->wheels.ptr, m * sizeof(rg::WheelRuntime), cudaMemcpyDeviceToHost),
+          "settled wheels");
+    check(cudaMemcpy(&ball, run->balls.ptr, sizeof(ball), cudaMemcpyDeviceToHost), "settled ball");
+    for (size_t i = 0; i < m; ++i) b->settle_rows_host.push_back(rg::KickoffSettledRow{cars[i], wheels[i]});
+    if (b->settle_ball_host.empty()) b->settle_ball_host.push_back(ball);
+}
+
+// Before a kickoff reset of a batch with kickoff_settled: every car slot's (config, team) entry, recording the new
+// ones, and the device copies the resets read (reference ensure_kickoff_settled, src/rocketgpu.cpp:1439-1500).
+void ensure_kickoff_settled(rg_batch* b, cudaStream_t s) {
+    if (!b->cfg.kickoff_settled || !b->settle_dirty) return;
+    const size_t n = static_cast<size_t>(b->env_count) * static_cast<size_t>(b->max_cars);
+    std::vector<rg::CarConfig> configs(n);
+    std::vector<uint8_t> teams(n);
+    if (n) {
+        check(cudaMemcpyAsync(configs.data(), b->car_cfgs.ptr, n * sizeof(rg::CarConfig), cudaMemcpyDeviceToHost, s),
+              "kickoff_settled configs");
+        check(cudaMemcpyAsync(teams.data(), b->teams.ptr, n, cudaMemcpyDeviceToHost, s), "kickoff_settled teams");
+        check(cudaStreamSynchronize(s), "kickoff_settled configs");
+    }
+    const int spawns = b->max_cars > 5 ? b->max_cars : 5;
+    std::vector<size_t> first;
+    std::vector<int32_t> entry(n);
+    const size_t old_entries = b->settle_entries.size(), old_rows = b->settle_rows_host.size(),
+                 old_balls = b->settle_ball_host.size();
+    try {
+        for (size_t i = 0; i < n; ++i) {
+            size_t e = 0;
+            while (e < b->settle_entries.size() &&
+                   !(b->settle_entries[e].team == teams[i] &&
+                     memcmp(&b->settle_entries[e].config, &configs[i], sizeof(rg::CarConfig)) == 0))
+                ++e;
+            if (e == b->settle_entries.size()) {
+                b->settle_entries.push_back(rg_batch::SettleEntry{configs[i], teams[i]});
+                first.push_back(i);
+            }
+            entry[i] = static_cast<int32_t>(e);
+        }
+        if (!first.empty()) record_kickoff_settled(b, first, configs, teams, spawns);
+    } catch (...) {
+        b->settle_entries.resize(old_entries);
+        b->settle_rows_host.resize(old_rows);
+        b->settle_ball_host.resize(old_balls);
+        throw;
+    }
+    const size_t m = b->settle_rows_host.size();
+    if (b->settle_rows.n != m) b->settle_rows.alloc(m);
+    check(cudaMemcpy(b->settle_rows.ptr, b->settle_rows_host.data(), m * sizeof(rg::KickoffSettledRow),
+                     cudaMemcpyHostToDevice),
+          "kickoff_settled rows");
+    if (b->settle_entry.n != n) b->settle_entry.alloc(n);
+    if (n) check(cudaMemcpy(b->settle_entry.ptr, entry.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice),
+                 "kickoff_settled entries");
+    if (!b->settle_ball_host.empty()) {
+        if (b->settle_ball.n != 1) b->settle_ball.alloc(1);
+        check(cudaMemcpy(b->settle_ball.ptr, b->settle_ball_host.data(), sizeof(rg::BallState),
+                         cudaMemcpyHostToDevice),
+              "kickoff_settled ball");
+    }
+    b->tc.settled_rows = b->settle_rows.ptr;
+    b->tc.settled_entry = b->settle_entry.ptr;
+    b->tc.settled_ball = b->settle_ball_host.empty() ? nullptr : b->settle_ball.ptr;
+    b->tc.settled_spawns = spawns;
+    b->settle_dirty = false;
+    b->drop_graphs();  // every captured launch holds the tick config
 }
 
 void launch_reset(rg_batch* b, uint64_t seed, cudaStream_t s) {
@@ -825,7 +974,7 @@ RG_API void rg_sim_config_default(rg_sim_config* c) {
     c->arena_restitution = 0.30f;
     c->goal_base_threshold_y = 5124.2373046875f;
     // the reference defaults to 1 (rocketgpu.h:831); this build has no kickoff settling and refuses 1
-    c->kickoff_settled = 0;
+    c->kickoff_settled = 1;
 }
 
 RG_API void rg_default_ball_state(rg_ball_state* o) {
@@ -1086,11 +1235,7 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         // arenas would need more, so they are refused rather than run with rows dropped.
         if (cfg->max_cars_per_env < 0 || cfg->max_cars_per_env > 6)
             throw std::invalid_argument("max_cars_per_env must be in [0, 6]");
-        // Kickoff settling (the reference's MutatorConfig::kickoff_settled, src/rocketgpu.cpp:1538-1603: kickoffs
-        // that start from a pre-recorded settle of the countdown) is not built: refuse it instead of resetting
-        // differently from the reference.
-        if (cfg->kickoff_settled != 0)
-            throw std::invalid_argument("kickoff_settled = 1 is not supported by this build; set it to 0");
+        if (cfg->kickoff_settled > 1) throw std::invalid_argument("kickoff_settled must be 0 or 1");
         if (!(cfg->tick_dt > 0.0f)) throw std::invalid_argument("tick_dt must be positive");
         std::unique_ptr<rg_batch> b(new rg_batch);
         b->device = device;
@@ -1212,7 +1357,19 @@ RG_API int rg_batch_create(const rg_sim_config* cfg, const rg_arena_layout* layo
         check(cudaMemcpy(b->env_car_count.ptr, b->host_car_count.data(), b->env_count * sizeof(int32_t),
                          cudaMemcpyHostToDevice),
               "upload car counts");
-        // BatchSim's constructor ends with reset_to_kickoff(0) (src/rocketgpu.cpp:1281)
+        if (cfg->kickoff_settled) {
+            // kept for the batches that record the settled kickoffs
+            b->layout_vertices.assign(layout->vertices_uu, layout->vertices_uu + 3 * layout->vertex_count);
+            b->layout_indices.assign(layout->indices, layout->indices + layout->index_count);
+            b->layout_has_rules = layout->rules != nullptr;
+            if (layout->rules) b->layout_rules = *layout->rules;
+            b->layout_has_pads = layout->boost_pads != nullptr;
+            if (layout->boost_pads)
+                b->layout_pads.assign(layout->boost_pads, layout->boost_pads + layout->boost_pad_count);
+        }
+        // BatchSim's constructor ends with reset_to_kickoff(0) (src/rocketgpu.cpp:1281), which records the settled
+        // kickoff of the default car first when settling is on
+        ensure_kickoff_settled(b.get(), nullptr);
         launch_reset(b.get(), 0, nullptr);
         check(cudaDeviceSynchronize(), "initial kickoff reset");
         *out = b.release();
@@ -1243,6 +1400,7 @@ RG_API int rg_batch_set_env_car_count(rg_batch* b, const int32_t* counts, size_t
         }
         DeviceGuard dg(b->device);
         std::memcpy(b->host_car_count.data(), counts, count * sizeof(int32_t));
+        b->settle_dirty = true;
         for (size_t i = 0; i < count; ++i) b->pads_live = b->pads_live || counts[i] > 0;
         rebuild_step_order(b, static_cast<cudaStream_t>(stream));
         check(cudaMemcpyAsync(b->env_car_count.ptr, counts, count * sizeof(int32_t), cudaMemcpyHostToDevice,
@@ -1386,6 +1544,7 @@ RG_API int rg_batch_set_car_configs(rg_batch* b, const rg_car_config* host, size
             if (host[i].three_wheels) throw std::invalid_argument("three-wheel car configs are not supported");
         upload_array(b, b->car_cfgs, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "set_car_configs",
                      stream);
+        b->settle_dirty = true;
     });
 }
 RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, void* stream) {
@@ -1393,12 +1552,14 @@ RG_API int rg_batch_set_teams(rg_batch* b, const uint8_t* host, size_t count, vo
         for (size_t i = 0; host && i < count; ++i)
             if (host[i] > 1) throw std::invalid_argument("team must be 0 (blue) or 1 (orange)");
         upload_array(b, b->teams, host, count, static_cast<size_t>(rg_batch_car_capacity(b)), "set_teams", stream);
+        b->settle_dirty = true;
     });
 }
 RG_API int rg_batch_reset_to_kickoff(rg_batch* b, uint64_t seed, void* stream) {
     return guard([&] {
         if (!b) throw std::invalid_argument("null argument");
         DeviceGuard dg(b->device);
+        ensure_kickoff_settled(b, static_cast<cudaStream_t>(stream));
         launch_reset(b, seed, static_cast<cudaStream_t>(stream));
     });
 }
@@ -1451,6 +1612,7 @@ RG_API int rg_batch_apply_env_commands(rg_batch* b, const rg_env_command* host, 
         if (active == 0) return;
         DeviceGuard dg(b->device);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
+        ensure_kickoff_settled(b, s);
         check(cudaMemcpyAsync(b->command_scratch.ptr, host, count * sizeof(rg_env_command), cudaMemcpyHostToDevice, s),
               "apply_env_commands upload");
         CarTickArgs a = car_tick_args(b, nullptr, 0);
@@ -1471,6 +1633,7 @@ RG_API int rg_batch_apply_env_commands_device(rg_batch* b, const rg_env_command*
             throw std::out_of_range("apply_env_commands_device count exceeds env_count");
         if (count == 0) return;
         DeviceGuard dg(b->device);
+        ensure_kickoff_settled(b, static_cast<cudaStream_t>(stream));
         CarTickArgs a = car_tick_args(b, nullptr, 0);
         a.pads = b->pads.ptr;
         apply_commands_kernel<<<(static_cast<int>(count) + 63) / 64, 64, 0, static_cast<cudaStream_t>(stream)>>>(
@@ -1492,6 +1655,7 @@ RG_API int rg_batch_step_with_device_commands(rg_batch* b, const rg_car_controls
             throw std::invalid_argument("control_stride must be zero or at least the total car capacity");
         if (command_stride < b->env_count) throw std::invalid_argument("env_command_stride must be at least env_count");
         DeviceGuard dg(b->device);
+        ensure_kickoff_settled(b, static_cast<cudaStream_t>(stream));
         step_car_path(b, reinterpret_cast<const rg::CarControls*>(device_controls), control_stride, ticks,
                       static_cast<cudaStream_t>(stream), reinterpret_cast<const rg::EnvCommand*>(device_commands),
                       command_stride);
@@ -1576,6 +1740,9 @@ RG_API int rg_batch_add_mesh(rg_batch* b, const rg_arena_layout* layout, int32_t
     return guard([&] {
         if (!b || !layout || !mesh_index) throw std::invalid_argument("null argument");
         if (b->extra_meshes.size() + 1 >= 255) throw std::out_of_range("a batch holds at most 255 meshes");
+        // the settled kickoffs are recorded on the batch's create-time geometry only
+        if (b->cfg.kickoff_settled)
+            throw std::invalid_argument("a batch with kickoff_settled = 1 takes no further geometry");
         rg::MeshHost h = rg::build_mesh_host(layout->vertices_uu, layout->vertex_count, layout->indices,
                                              layout->index_count);
         DeviceGuard dg(b->device);

@@ -225,6 +225,45 @@ RG_HDI void prefer_kickoff_spot_for_short_team(int* order, int team_count, const
 
 // How a kickoff reset treats the match (the EnvCommand fields of the reference's ResetEnvToKickoff call,
 // env_step.hpp:5735-5752). The defaults are BatchSim::reset_to_kickoff's: a new match.
+// A car's state at its kickoff spot once the game's countdown has run, with its wheel record (reference
+// KickoffSettledRow, arena_geometry.hpp:1580-1583).
+struct KickoffSettledRow {
+    CarState car;
+    WheelRuntime wheels;
+};
+// A non-countdown kickoff puts each car (whose config and team have a recorded entry) into the recorded state of its
+// spot, keeping the car's event and touch history (reference SettleKickoffCar and the kickoff history fields,
+// arena_ball.hpp:2698-2767; the CPU build's word copy takes every other byte, driving_disabled included).
+RG_HDI void settle_kickoff_car(CarState& c, WheelRuntime& w, int32_t entry, int spot, const TickConfig& tc) {
+    if (tc.settled_rows == nullptr || spot >= tc.settled_spawns || entry < 0) return;
+    const KickoffSettledRow& row = tc.settled_rows[static_cast<size_t>(entry) * tc.settled_spawns + spot];
+    uint8_t bumps[7], demos[7];
+    memcpy(bumps, c.bump_event_bumps, sizeof(bumps));
+    memcpy(demos, c.bump_event_demos, sizeof(demos));
+    const uint64_t prev_ball = c.previous_ball_contact_start, last_ball = c.last_ball_contact_start,
+                   last_world = c.last_world_surface_contact, world_after_prev = c.first_world_after_previous_ball,
+                   world_after_last = c.first_world_after_last_ball, flip_or_jump = c.last_flip_or_jump_start,
+                   dir_flip = c.last_directional_flip_start, touch_tick = c.latest_touch_tick;
+    const uint8_t started_with_world = c.last_ball_started_with_world, foj_last = c.flip_or_jump_last_tick;
+    const V3 touch_loc = c.latest_touch_location, touch_normal = c.latest_touch_normal;
+    c = row.car;
+    memcpy(c.bump_event_bumps, bumps, sizeof(bumps));
+    memcpy(c.bump_event_demos, demos, sizeof(demos));
+    c.previous_ball_contact_start = prev_ball;
+    c.last_ball_contact_start = last_ball;
+    c.last_world_surface_contact = last_world;
+    c.first_world_after_previous_ball = world_after_prev;
+    c.first_world_after_last_ball = world_after_last;
+    c.last_flip_or_jump_start = flip_or_jump;
+    c.last_directional_flip_start = dir_flip;
+    c.last_ball_started_with_world = started_with_world;
+    c.flip_or_jump_last_tick = foj_last;
+    c.latest_touch_tick = touch_tick;
+    c.latest_touch_location = touch_loc;
+    c.latest_touch_normal = touch_normal;
+    w = row.wheels;
+}
+
 struct KickoffReset {
     bool preserve_score = false;  // keep scores, tick and last scorer; with seed 0, the match's next kickoff
     uint8_t seed_mode = 0;        // 0: spot order from the seed (0: from the reset count); 2: as 0 with seed 0;
@@ -244,10 +283,12 @@ RG_HD int reset_visit_slot(const EnvState& env, int k, int count) {
 // arena_ball.hpp:2846-3085, with no platform respawn RNG, no settled-kickoff copy and no countdown). `teams` are the
 // arena's max_cars slot teams (0 blue, 1 orange); `scratch` is its persistent ball contact state, cleared as the
 // reference clears its solver scratch.
+// wheels and settled_entry (the arena's slots' settle entries, null when settling is off) are the arena's.
 RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, BallState& ball, BallWorldScratch& scratch,
-                                 CarState* cars, const CarConfig* cfgs, CarControls* controls, PadState* pads,
-                                 const PadLayout& L, const uint8_t* teams, int count, int max_cars,
-                                 const TickConfig& tc, const KickoffReset& how = KickoffReset{}) {
+                                 CarState* cars, WheelRuntime* wheels, const CarConfig* cfgs, CarControls* controls,
+                                 PadState* pads, const PadLayout& L, const uint8_t* teams, int count, int max_cars,
+                                 const TickConfig& tc, const int32_t* settled_entry,
+                                 const KickoffReset& how = KickoffReset{}) {
     memset(&scratch, 0, sizeof(scratch));
     const EnvState saved = env;
     EnvState next;
@@ -321,6 +362,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
         for (int i = 0; i < 5; ++i) order_bits[t] |= static_cast<uint32_t>(team_order[t][i]) << (3 * i);
 
     reset_kickoff_ball(ball, rules, how.game_spawn);
+    if (!how.game_spawn && tc.settled_rows != nullptr && tc.settled_ball != nullptr) ball = *tc.settled_ball;
     if (pads && !how.keep_pads) {
         for (int p = 0; p < L.count; ++p) {
             PadState& pad = pads[p];
@@ -358,6 +400,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
             if (nth >= 5) pos = pos - V3{game_cosf(yaw), game_sinf(yaw), 0.0f} * step;
             place_car_at_world_spawn(cars[i], pos, yaw, cfgs[i].spawn_z, tc.boost_spawn_amount);
             if (how.game_spawn && nth < 5) pend_kickoff_spawn(cars[i], spot, tc.tick_dt);
+            if (!how.game_spawn && settled_entry) settle_kickoff_car(cars[i], wheels[i], settled_entry[i], spot, tc);
             continue;
         }
         SpawnPos spawn;
@@ -373,6 +416,7 @@ RG_HDI void reset_env_to_kickoff(int env_idx, uint64_t seed, EnvState& env, Ball
         }
         place_car_at_kickoff_spawn(cars[i], team, spawn, cfgs[i].spawn_z, tc.boost_spawn_amount);
         if (how.game_spawn && nth < 5) pend_kickoff_spawn(cars[i], spot, tc.tick_dt);
+        if (!how.game_spawn && settled_entry) settle_kickoff_car(cars[i], wheels[i], settled_entry[i], spot, tc);
     }
 }
 

@@ -282,6 +282,8 @@ RG_API int rg_server_open(const rg_server_config* scfg, const rg_sim_config* sim
             throw std::invalid_argument("give max_arenas or hbm_budget_bytes");
         if (sim->max_cars_per_env <= 0 || sim->max_cars_per_env > 6)
             throw std::invalid_argument("max_cars_per_env must be in [1, 6]");
+        // a client's kickoffs run in the pool's slots without the batch's settle entries
+        if (sim->kickoff_settled != 0) throw std::invalid_argument("the server takes kickoff_settled = 0");
         std::unique_ptr<rg_server> s(new rg_server);
         s->device = device;
         s->policy = scfg->policy;

@@ -70,6 +70,8 @@ struct ArenaRules {
     V3 goal_point[2], goal_normal[2], goal_min[2], goal_max[2];
 };
 
+struct KickoffSettledRow;  // rg_reset.cuh
+
 struct TickConfig {
     float tick_dt;
     float gravity_z;
@@ -100,6 +102,12 @@ struct TickConfig {
     float bump_force_scale, bump_cooldown_time;
     uint64_t kickoff_seed;  // the last reset_to_kickoff seed: demolished cars' respawn draw (reference Impl::seed)
     const ArenaRules* rules;  // custom spawns and goals (memory the kernels can read), or null
+    // Kickoff settling (reference SimConfig::kickoff_settled_*, rocketgpu.h:892-897): per (car config, team) entry
+    // and kickoff spot, the car and wheel record the game's countdown leaves, and the ball it leaves; null when off.
+    const KickoffSettledRow* settled_rows;
+    const int32_t* settled_entry;  // per car slot: its entry, or -1
+    const BallState* settled_ball;
+    int32_t settled_spawns;  // rows per entry (kickoff spots): max(max_cars_per_env, 5)
 };
 
 }  // namespace rg

@@ -284,6 +284,7 @@ struct ArenaCars {
     const CarControls* controls;
     const uint8_t* teams;
     CarCarManifold* pairs;  // the arena's retained car-car manifolds, slot car_pair_slot(lo, hi)
+    const int32_t* settled_entry;  // the slots' kickoff-settle entries, or null (settling off)
     int count, max_cars, car_base;
 };
 
@@ -1813,8 +1814,8 @@ RG_HDI void apply_env_command(const EnvCommand& cmd, int env_idx, EnvState& env,
     how.seed_mode = cmd.kickoff_seed_mode;
     how.keep_pads = cmd.keep_boost_pads != 0;
     how.game_spawn = cmd.kickoff_countdown_ticks != 0;
-    reset_env_to_kickoff(env_idx, cmd.kickoff_seed, env, ball, *cs.ball_world, A.cars, A.cfgs, controls, A.pads, L,
-                         A.teams, count, A.max_cars, tc, how);
+    reset_env_to_kickoff(env_idx, cmd.kickoff_seed, env, ball, *cs.ball_world, A.cars, A.wheels, A.cfgs, controls,
+                         A.pads, L, A.teams, count, A.max_cars, tc, A.settled_entry, how);
     clear_retained_car_contacts(cs, A.max_cars);
     // the countdown: driving off for its ticks (or until the game timers end it), the ball held in its plane
     // (reference ApplyEnvCommand, env_step.hpp:5747-5752)

@@ -41,7 +41,7 @@ class Server:
         lay.indices = self._i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
         lay.index_count = len(self._i)
         cfg = abi.rg_server_config(max_arenas, self.POLICIES[policy], hbm_budget_bytes)
-        sim = SimConfig(env_count=1, max_cars_per_env=max_cars_per_env, **sim_kw)
+        sim = SimConfig(env_count=1, max_cars_per_env=max_cars_per_env, **{"kickoff_settled": 0, **sim_kw})
         h = ctypes.c_void_p()
         _call(abi.lib().rg_server_open(ctypes.byref(cfg), ctypes.byref(sim.c), ctypes.byref(lay), device,
                                        ctypes.byref(h)))

@@ -83,8 +83,8 @@ def test_invalid_config_is_rejected_before_any_device_call(arena_mesh):
     with pytest.raises(ValueError):
         BatchSim(SimConfig(env_count=4, max_cars_per_env=7), v, i)
     with pytest.raises(ValueError, match="kickoff_settled"):
-        BatchSim(SimConfig(env_count=4, kickoff_settled=1), v, i)
-    assert SimConfig().c.kickoff_settled == 0
+        BatchSim(SimConfig(env_count=4, kickoff_settled=2), v, i)
+    assert SimConfig().c.kickoff_settled == 1  # the reference's default
     with pytest.raises(ValueError):
         BatchSim(SimConfig(env_count=4), v, i[:-1])
     bad = v.copy()
@@ -143,11 +143,11 @@ def test_pybind_module_mirrors_the_reference_binding(arena_mesh):
         assert hasattr(layout, name), name
     assert layout.goals[1].point.y == layout.goals[1].point.y and len(layout.respawn_spawns[1]) == 4
     cfg = m.SimConfig()
-    assert cfg.kickoff_settled == 0 and cfg.max_cars_per_env == 6
+    assert cfg.kickoff_settled == 1 and cfg.max_cars_per_env == 6
     v, i = arena_mesh
     layout = m.ArenaLayout()
     layout.meshes = [m.ArenaMesh(v, i)]
-    cfg.kickoff_settled = 1
+    cfg.kickoff_settled = 2
     with pytest.raises(ValueError, match="kickoff_settled"):
         m.BatchSim(cfg, layout)
     cfg.kickoff_settled = 0

@@ -31,7 +31,7 @@ def test_two_geometries_in_one_batch(oracle_available, arena_mesh):
         o.set_teams(teams)
         o.reset_to_kickoff(17)
         orcs.append(o)
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), *meshes[0])
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), *meshes[0])
     assert gpu.add_mesh(*meshes[1]) == 1
     gpu.set_arena_meshes(mesh_of)
     gpu.set_env_car_count(counts)

@@ -56,19 +56,19 @@ def test_layout_rules_and_pads_are_validated_before_any_device_call(arena_mesh):
     r = arena_rules()
     r.kickoff_spawns[0][1].yaw = 30.0  # beyond 8 pi
     with pytest.raises(ValueError, match="yaw"):
-        BatchSim(SimConfig(env_count=2), v, i, rules=r)
+        BatchSim(SimConfig(kickoff_settled=0, env_count=2), v, i, rules=r)
     r = arena_rules()
     r.goals[1].min.y = float("nan")
     with pytest.raises(ValueError, match="NaN"):
-        BatchSim(SimConfig(env_count=2), v, i, rules=r)
+        BatchSim(SimConfig(kickoff_settled=0, env_count=2), v, i, rules=r)
     r = arena_rules()
     r.ball_spawn.x = 12000.0
     with pytest.raises(ValueError, match="ball spawn"):
-        BatchSim(SimConfig(env_count=2), v, i, rules=r)
+        BatchSim(SimConfig(kickoff_settled=0, env_count=2), v, i, rules=r)
     with pytest.raises(ValueError, match="kMaxBoostPads"):
-        BatchSim(SimConfig(env_count=2), v, i, boost_pads=[(0.0, 0.0, 70.0, 0)] * 49)
+        BatchSim(SimConfig(kickoff_settled=0, env_count=2), v, i, boost_pads=[(0.0, 0.0, 70.0, 0)] * 49)
     with pytest.raises(ValueError, match="boost pad position"):
-        BatchSim(SimConfig(env_count=2), v, i, boost_pads=[(0.0, float("inf"), 70.0, 0)])
+        BatchSim(SimConfig(kickoff_settled=0, env_count=2), v, i, boost_pads=[(0.0, float("inf"), 70.0, 0)])
 
 
 def _run(arena_mesh, rules, pads, n, ticks, seed):
@@ -83,7 +83,7 @@ def _run(arena_mesh, rules, pads, n, ticks, seed):
     orc = oracle_ref.OracleSim(n, MC, v, i, kickoff_settled=False,
                                rules=None if rules is None else _rules_floats(rules),
                                pad_layout=None if pads is None else np.array(pads, np.float32))
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i, rules=rules, boost_pads=pads)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i, rules=rules, boost_pads=pads)
     assert gpu.pad_capacity() == orc.pad_capacity
     for sim in (orc, gpu):
         sim.set_env_car_count(counts)

@@ -16,7 +16,7 @@ def _pair(n, arena_mesh):
     v, i = arena_mesh
     orc = oracle_ref.OracleSim(n, 2, v, i, kickoff_settled=False)
     orc.set_env_car_count([0] * n)
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=2), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=2), v, i)
     gpu.set_env_car_count([0] * n)
     return orc, gpu
 
@@ -76,7 +76,7 @@ def test_golden_free_flight(arena_mesh):
     g = np.load(os.path.join(HERE, "golden", "ball_free_flight.npz"))
     v, i = arena_mesh
     n = g["init_balls"].shape[0]
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=2), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=2), v, i)
     gpu.set_env_car_count([0] * n)
     gpu.upload_ball_states(g["init_balls"])
     gpu.upload_env_states(g["init_envs"])
@@ -126,7 +126,7 @@ def test_golden_contacts(arena_mesh):
     g = np.load(os.path.join(HERE, "golden", "ball_contacts.npz"))
     v, i = arena_mesh
     n = g["init_balls"].shape[0]
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=2), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=2), v, i)
     gpu.set_env_car_count([0] * n)
     gpu.upload_ball_states(g["init_balls"])
     gpu.upload_env_states(g["init_envs"])

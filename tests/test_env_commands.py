@@ -29,7 +29,7 @@ def _pair(n, arena_mesh, counts, teams, seed):
     from rocketgpu_b200.batch_sim import BatchSim, SimConfig
     v, i = arena_mesh
     orc = oracle_ref.OracleSim(n, MC, v, i, kickoff_settled=False)
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i)
     for sim in (orc, gpu):
         sim.set_env_car_count(counts)
         sim.set_teams(teams)

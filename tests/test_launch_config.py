@@ -17,7 +17,7 @@ def _run(arena_mesh, config, steps=24, n=512):
     v, i = arena_mesh
     rng = np.random.default_rng(3)
     counts = rng.choice(np.array([2, 4, 6], np.int32), size=n, p=[0.55, 0.27, 0.18]).astype(np.int32)
-    sim = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i)
+    sim = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i)
     sim.set_env_car_count(counts)
     sim.reset_to_kickoff(3)
     if config is not None:
@@ -51,7 +51,7 @@ def test_autotune_picks_a_candidate(arena_mesh):
     from rocketgpu_b200.batch_sim import BatchSim, SimConfig
     v, i = arena_mesh
     n = 256
-    sim = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i)
+    sim = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i)
     sim.set_env_car_count(np.full(n, 4, np.int32))
     sim.reset_to_kickoff(1)
     ctrl = torch.zeros((8 * n * MC, 24), dtype=torch.uint8, device="cuda")

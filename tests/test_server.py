@@ -33,7 +33,7 @@ def _alone(arena_mesh, spec):
     counts, teams, cfgs, seed, reqs = spec
     n = len(counts)
     v, i = arena_mesh
-    sim = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i)
+    sim = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i)
     sim.set_env_car_count(counts)
     sim.set_teams(teams)
     sim.set_car_configs(cfgs)

@@ -27,7 +27,7 @@ def test_state_arrays_by_name_and_device_arrays(oracle_available, arena_mesh):
     v, i = arena_mesh
     n = 64
     orc = oracle_ref.OracleSim(n, MC, v, i, kickoff_settled=False)
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=MC), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=MC), v, i)
     for sim in (orc, gpu):
         sim.set_env_car_count([2] * n)
         sim.set_teams(np.tile(np.array([0, 1], np.uint8), n))
@@ -86,7 +86,7 @@ def test_internal_state_snapshot_restores_a_batch(arena_mesh):
     from rocketgpu_b200.batch_sim import BatchSim, SimConfig
     v, i = arena_mesh
     n, mc = 48, 4
-    gpu = BatchSim(SimConfig(env_count=n, max_cars_per_env=mc), v, i)
+    gpu = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=mc), v, i)
     counts = np.array([2, 4, 3] * (n // 3), np.int32)
     gpu.set_env_car_count(counts)
     gpu.set_teams(np.tile(np.array([0, 1, 0, 1], np.uint8), n))
@@ -137,7 +137,7 @@ def test_pybind_module_steps_like_the_oracle(oracle_available, arena_mesh):
     v, i = arena_mesh
     n, mc = 32, 6
     cfg = m.SimConfig()
-    cfg.env_count, cfg.max_cars_per_env = n, mc
+    cfg.env_count, cfg.max_cars_per_env, cfg.kickoff_settled = n, mc, 0
     layout = m.ArenaLayout()
     layout.meshes = [m.ArenaMesh(v, i)]
     sim = m.BatchSim(cfg, layout)

@@ -27,7 +27,7 @@ def test_static_scratch_step_matches_batch_step_on_two_calls(arena_mesh):
     lib = abi.lib()
     v, i = arena_mesh
     n = 1024
-    ref = BatchSim(SimConfig(env_count=n, max_cars_per_env=2), v, i)
+    ref = BatchSim(SimConfig(kickoff_settled=0, env_count=n, max_cars_per_env=2), v, i)
     ref.set_env_car_count([0] * n)
     default_ball = np.zeros(288, np.uint8)
     lib.rg_default_ball_state(default_ball.ctypes.data)
@@ -64,7 +64,7 @@ def test_static_scratch_rejects_too_many_arenas(arena_mesh):
 
     lib = abi.lib()
     v, i = arena_mesh
-    sim = BatchSim(SimConfig(env_count=8, max_cars_per_env=2), v, i)
+    sim = BatchSim(SimConfig(kickoff_settled=0, env_count=8, max_cars_per_env=2), v, i)
     d = torch.zeros(16, dtype=torch.uint8, device="cuda")
     rc = lib.rg_batch_step_static_scratch(sim._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()),
                                           4097, 1, 1, None)
