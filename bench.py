@@ -82,9 +82,10 @@ KERNEL_BYTES = {
     "arena_tail": (2 * (288 + 44 + 34 * 16), 2 * 880 + 120, 0),
 }
 KERNEL_NAMES = ("arena_begin", "car_pre", "car_vehicle", "arena_finish", "car_post", "arena_tail")
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the dominant kernel at 16,384 arenas,
-# from the ncu capture summarised in profiles/ (a smaller capture scaled by arenas); None until captured.
-KERNEL_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per car of one car_vehicle_kernel launch, from an ncu
+# --set full capture of the mixed workload at 4,096 arenas (13,350 cars: 31.01 MB read + 13.92 MB written); a launch
+# at the bench's size is scaled by its cars (the kernel's traffic is per car: its state, stage and mesh reads).
+KERNEL_TRAFFIC_PER_CAR = {"car_vehicle": (31.014656e6 + 13.916416e6) / 13350}
 
 
 def peaks():
@@ -481,7 +482,9 @@ def run_ours(args, world, rank, local):
         line["roofline"] = {
             "bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_source": peak_kind,
-            "traffic": KERNEL_TRAFFIC.get(top),
+            "traffic": KERNEL_TRAFFIC_PER_CAR[top] * cars_total if top in KERNEL_TRAFFIC_PER_CAR else None,
+            "traffic_note": "car_vehicle_kernel alone (the phase also holds car_rays_kernel), 4,096-arena ncu capture "
+                            "scaled by cars",
             "algorithmic_bytes_per_launch": top_bytes, "avg_launch_ms": per_launch_ms[top],
             "note": "dominant kernel by device time; the tick is bound by latency and FP32 issue of serial per-arena "
                     "work, not by HBM; frac is the HBM fraction of its algorithmic state bytes"}
