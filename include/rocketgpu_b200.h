@@ -168,6 +168,23 @@ typedef struct rg_env_command {
     uint64_t kickoff_seed;
 } rg_env_command;
 
+/* reference PhysicsEvent / PhysicsEventWindow (rocketgpu.h:44-70; types: 0 ball touch start, 1 ball-world contact,
+ * 2 car-world contact, 3 boost pickup, 4 car bump, 5 goal). Fields an event does not set are 0, team -1. */
+typedef struct rg_physics_event {
+    uint64_t tick;
+    uint8_t type;
+    uint32_t car_id, other_car_id;
+    int32_t team;
+    uint32_t pad_index;
+    uint8_t car_on_ground, is_big_pad, is_demo;
+    rg_vec3 position, normal, car_velocity, ball_position, ball_velocity;
+    float boost_before, boost_after;
+} rg_physics_event;
+typedef struct rg_physics_event_window {
+    uint64_t tick;
+    uint32_t count, overflow;
+} rg_physics_event_window;
+
 /* The BatchSim configuration subset this path takes (reference SimConfig, rocketgpu.h:842-909, and the
  * MutatorConfig fields the tick reads, rocketgpu.h:708-840). Zero-initialise, then call rg_sim_config_default. */
 typedef struct rg_sim_config {
@@ -345,6 +362,14 @@ RG_API int rg_batch_phase_times(rg_batch* b, float* out_ms, int64_t* out_ticks);
 
 /* BatchSim::synchronize (rocketgpu.h:1083). Also reports a CUDA error from an earlier launch. */
 RG_API int rg_batch_synchronize(rg_batch* b, void* stream);
+
+/* BatchSim::set_physics_event_stream (rocketgpu.h:1015; src/rocketgpu.cpp:2896-2906, in the Python binding's form,
+ * python/rocketgpu_bindings.cpp:832-845): device arrays records[env_count * capacity_per_env] and windows[env_count].
+ * Every tick stamps each arena's window with its tick and appends that tick's events in the reference's order; a full
+ * window sets overflow. The caller clears the counts between reads. goal_only keeps goals only. Null arrays and 0
+ * turn the stream off. Synchronise before freeing the arrays (captured step graphs are dropped here). */
+RG_API int rg_batch_set_physics_event_stream(rg_batch* b, rg_physics_event* records, rg_physics_event_window* windows,
+                                             uint32_t capacity_per_env, int32_t goal_only);
 
 /* Arenas on different geometries in one batch. The reference takes one geometry per BatchSim (ArenaLayout,
  * rocketgpu.h:943-959), so a mix of arenas needs one BatchSim per mesh there; here one batch holds up to 255 meshes.

@@ -197,6 +197,30 @@ int orc_step_with_commands(void* h, const void* ctrl, int32_t ctrl_stride, const
     });
 }
 
+// BatchSim::set_physics_event_stream with host arrays (the CPU build writes them directly): records[env * capacity + k],
+// windows[env]; capacity 0 and null arrays turn the stream off. Also reports the struct sizes the checker reads.
+int orc_set_physics_event_stream(void* h, void* records, void* windows, uint32_t capacity, int goal_only) {
+    return Guard([&] {
+        PhysicsEventStream s;
+        s.records = static_cast<PhysicsEvent*>(records);
+        s.windows = static_cast<PhysicsEventWindow*>(windows);
+        s.capacity_per_env = capacity;
+        if (records || windows || capacity) {
+            s.goal_only = goal_only != 0;
+            s.env_count = static_cast<uint32_t>(ORC_SIM->env_count());
+            s.cars_per_env = static_cast<uint32_t>(ORC_SIM->car_capacity() / ORC_SIM->env_count());
+        }
+        ORC_SIM->set_physics_event_stream(s);
+    });
+}
+int orc_physics_event_sizes(int64_t* out) {
+    out[0] = sizeof(PhysicsEvent);
+    out[1] = sizeof(PhysicsEventWindow);
+    out[2] = offsetof(PhysicsEvent, position);
+    out[3] = offsetof(PhysicsEvent, boost_after);
+    return 0;
+}
+
 int orc_download_cars(void* h, void* out, int64_t n) {
     return Guard([&] { ORC_SIM->download_car_states(static_cast<CarState*>(out), (size_t)n); });
 }

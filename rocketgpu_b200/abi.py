@@ -17,6 +17,7 @@ EXPORTS = [
     "rg_batch_create", "rg_batch_destroy", "rg_batch_env_count", "rg_batch_car_capacity",
     "rg_batch_set_env_car_count", "rg_batch_upload_ball_states", "rg_batch_download_ball_states",
     "rg_batch_upload_env_states", "rg_batch_download_env_states", "rg_batch_step", "rg_batch_synchronize",
+    "rg_batch_set_physics_event_stream",
     "rg_batch_device_view", "rg_ucrt_sinf", "rg_ucrt_cosf", "rg_ucrt_atan2f", "rg_ucrt_powf",
     "rg_arena_mesh_tables", "rg_batch_step_static_scratch",
     "rg_default_car_state", "rg_default_car_config", "rg_batch_upload_car_states", "rg_batch_download_car_states",
@@ -127,6 +128,7 @@ def lib():
             getattr(L, n).argtypes = [vp, vp, sz, vp]
         L.rg_batch_step.argtypes = [vp, i32, vp]
         L.rg_batch_synchronize.argtypes = [vp, vp]
+        L.rg_batch_set_physics_event_stream.argtypes = [vp, vp, vp, ctypes.c_uint32, i32]
         L.rg_batch_device_view.argtypes = [vp, vp]
         for n in ("rg_ucrt_sinf", "rg_ucrt_cosf"):
             getattr(L, n).argtypes = [ctypes.c_float]

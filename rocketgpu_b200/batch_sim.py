@@ -75,6 +75,19 @@ class SimConfig:
         self.c = c
 
 
+# rg_physics_event / rg_physics_event_window as numpy records (reference PhysicsEvent / PhysicsEventWindow).
+_V3 = (np.float32, (3,))
+PHYSICS_EVENT_DTYPE = np.dtype({
+    "names": ["tick", "type", "car_id", "other_car_id", "team", "pad_index", "car_on_ground", "is_big_pad", "is_demo",
+              "position", "normal", "car_velocity", "ball_position", "ball_velocity", "boost_before", "boost_after"],
+    "formats": [np.uint64, np.uint8, np.uint32, np.uint32, np.int32, np.uint32, np.uint8, np.uint8, np.uint8,
+                _V3, _V3, _V3, _V3, _V3, np.float32, np.float32],
+    "offsets": [0, 8, 12, 16, 20, 24, 28, 29, 30, 32, 44, 56, 68, 80, 92, 96],
+    "itemsize": 104})
+PHYSICS_EVENT_WINDOW_DTYPE = np.dtype([("tick", np.uint64), ("count", np.uint32), ("overflow", np.uint32)])
+EVENT_TYPES = ("ball_touch_start", "ball_world_contact", "car_world_contact", "boost_pickup", "car_bump", "goal")
+
+
 class BatchSim:
     """N independent arenas on one GPU, stepped by whole 120 Hz ticks.
 
@@ -232,6 +245,13 @@ class BatchSim:
 
     def synchronize(self, stream: int = 0):
         _check(abi.lib().rg_batch_synchronize(self._h, stream))
+
+    def set_physics_event_stream(self, records: int, windows: int, capacity: int, goal_only: bool = False):
+        """BatchSim::set_physics_event_stream (reference rocketgpu.h:1015, in the Python binding's form): device
+        pointers to records[env_count * capacity] (PHYSICS_EVENT_DTYPE) and windows[env_count]
+        (PHYSICS_EVENT_WINDOW_DTYPE); zeros turn the stream off."""
+        _check(abi.lib().rg_batch_set_physics_event_stream(self._h, records or None, windows or None, capacity,
+                                                           1 if goal_only else 0))
 
     def device_view(self) -> dict:
         v = abi.rg_device_view()

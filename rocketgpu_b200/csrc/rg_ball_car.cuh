@@ -504,9 +504,10 @@ RG_HDI V3 quat_inverse_rotate(Q4 q, V3 v) {
 // Bookkeeping of a car's ball touch: touch start, the hit record and the game's extra hit impulse
 // (reference CommitBallCarHit). `car_pos` / `car_rot` / `ball_pos`: the bodies at the world step's start;
 // `car_start_vel` / `ball_start_vel`: their velocities at the tick start (uu).
+// A touch start is a ball-touch event of the car (team `team`) when `events` is on (reference :1216-1227).
 RG_HDI void commit_ball_hit(BallState& b, CarState& c, uint32_t car_id, uint64_t env_tick, V3 normal, V3 rel_ball_uu,
                             V3 rel_car_uu, V3 car_pos, Q4 car_rot, V3 ball_pos, V3 car_start_vel,
-                            V3 ball_start_vel) {
+                            V3 ball_start_vel, uint8_t team, const EventStream& events) {
     const bool started = !c.ball_contact_last_tick && !c.ball_contact_this_tick;
     if (started) {
         c.previous_ball_contact_start = c.last_ball_contact_start;
@@ -519,6 +520,17 @@ RG_HDI void commit_ball_hit(BallState& b, CarState& c, uint32_t car_id, uint64_t
         c.latest_touch_normal = normal;
     }
     c.ball_contact_this_tick = 1;
+    if (started && events.windows) {
+        PhysicsEvent e = new_event(kEventBallTouchStart);
+        e.car_id = car_id;
+        e.team = team;
+        e.car_on_ground = c.is_on_ground;
+        e.position = c.pos;
+        e.car_velocity = c.vel;
+        e.ball_position = b.pos;
+        e.ball_velocity = b.vel;
+        emit_event_for_car(events, car_id, e);
+    }
     BallHitInfo& h = c.ball_hit_info;
     const uint8_t had_prior = h.is_valid;
     const uint64_t prev_extra = h.tick_count_when_extra_impulse_applied;
@@ -554,7 +566,7 @@ RG_HDI void commit_ball_hit(BallState& b, CarState& c, uint32_t car_id, uint64_t
 // The hit from the retained manifold's averaged point (reference CommitBallCarHitFromManifold).
 RG_HDI void commit_ball_hit_from_manifold(BallState& b, CarState& c, const BallCarScratch& m, uint32_t car_id,
                                           uint64_t env_tick, V3 car_pos, Q4 car_rot, V3 ball_pos, V3 car_start_vel,
-                                          V3 ball_start_vel) {
+                                          V3 ball_start_vel, uint8_t team, const EventStream& events) {
     if (m.count == 0) return;
     V3 pa{0.0f, 0.0f, 0.0f}, pb{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
     for (int k = 0; k < m.count; ++k) {
@@ -564,6 +576,7 @@ RG_HDI void commit_ball_hit_from_manifold(BallState& b, CarState& c, const BallC
     }
     const float inv = 1.0f / static_cast<float>(m.count);
     commit_ball_hit(b, c, car_id, env_tick, ue3_safe_normal(n * inv), (pa * inv - b.pos_bt) * 50.0f,
-                    (pb * inv - c.pos_bt) * 50.0f, car_pos, car_rot, ball_pos, car_start_vel, ball_start_vel);
+                    (pb * inv - c.pos_bt) * 50.0f, car_pos, car_rot, ball_pos, car_start_vel, ball_start_vel, team,
+                    events);
 }
 }  // namespace rg

@@ -726,8 +726,10 @@ RG_HDI bool ball_predictive_hit(const BallState& b, const MeshDevice& m, float d
 // Builds the ball's mesh manifold and its contact rows for this tick (the mesh branch of
 // AppendBallWorldSpecialContactRows). `solver_vel_bt` is the ball's linear velocity the solver starts from;
 // `ext_delta` the external (gravity) velocity change in uu/s.
+// event_env >= 0: each triangle the ball meets is a ball-world event of that arena, with the triangle's own normal
+// (reference AppendBallWorldSpecialContactRows, arena_ball.hpp:1927-1936, 2195-2240).
 RG_NOINL void ball_mesh_contacts(const BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& m,
-                               V3 ext_delta, V3 solver_vel_bt, float dt, BallContactRows& rows) {
+                               V3 ext_delta, V3 solver_vel_bt, float dt, BallContactRows& rows, int event_env = -1) {
     const float radius_bt = c.ball_radius * (1.0f / 50.0f);
     const float threshold = (radius_bt + 0.08f) * 0.02f;
     const float rwt = radius_bt + threshold;
@@ -741,6 +743,14 @@ RG_NOINL void ball_mesh_contacts(const BallState& b, BallWorldScratch& s, const 
             V3 n, on_tri;
             float pen_uu, depth;
             if (!sphere_triangle(center, radius_bt, threshold, t.a, t.b, t.c, n, pen_uu, on_tri, depth)) return;
+            if (event_env >= 0 && c.events.windows) {
+                PhysicsEvent e = new_event(kEventBallWorldContact);
+                e.position = b.pos;
+                e.normal = n;
+                e.ball_position = b.pos;
+                e.ball_velocity = b.vel;
+                emit_event(c.events, static_cast<uint32_t>(event_env), e);
+            }
             const V3 on_a = on_tri + n * depth;
             const V3 rel = on_a - center;
             BallManifoldPt p;

@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256) tick_kernel(TickArgs a, int ticks) {
     rg::BallWorldScratch s = a.ball_world[e];
     const rg::MeshDevice& mesh = arena_mesh(a, e);
     for (int t = 0; t < ticks; ++t) {
-        rg::arena_tick(env, b, s, a.tc, mesh);
+        rg::arena_tick(env, b, s, a.tc, mesh, e);
     }
     a.balls[e] = b;
     a.envs[e] = env;
@@ -1736,6 +1736,28 @@ RG_API int rg_batch_synchronize(rg_batch* b, void* stream) {
         if (!b) throw std::invalid_argument("null argument");
         DeviceGuard dg(b->device);
         check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
+    });
+}
+
+RG_API int rg_batch_set_physics_event_stream(rg_batch* b, rg_physics_event* records, rg_physics_event_window* windows,
+                                             uint32_t capacity_per_env, int32_t goal_only) {
+    return guard([&] {
+        if (!b) throw std::invalid_argument("null argument");
+        const bool off = !records && !windows && capacity_per_env == 0;
+        if (!off && (!records || !windows || capacity_per_env == 0))
+            throw std::invalid_argument("physics event stream must match the complete batch");
+        DeviceGuard dg(b->device);
+        rg::EventStream es{};
+        if (!off) {
+            es.records = reinterpret_cast<rg::PhysicsEvent*>(records);
+            es.windows = reinterpret_cast<rg::PhysicsEventWindow*>(windows);
+            es.capacity = capacity_per_env;
+            es.env_count = static_cast<uint32_t>(b->env_count);
+            es.cars_per_env = static_cast<uint32_t>(b->max_cars);
+            es.goal_only = goal_only ? 1u : 0u;
+        }
+        b->tc.events = es;
+        b->drop_graphs();  // every captured launch holds the tick config
     });
 }
 

@@ -881,12 +881,26 @@ RG_HDI void demolish_car(CarState& c, const TickConfig& tc) {
     c.is_demoed = 1;
     c.demo_respawn_timer = tc.demo_respawn_time + tc.tick_dt;
 }
-RG_HDI void record_car_hit(CarState& hitter, uint32_t hitter_id, uint32_t victim_id, bool is_demo) {
+// The hitter's bump / demolition counters, and the car-bump event (reference RecordCarHit and the CarBump emits
+// beside it, triangle_and_carcar.hpp:2883-2895, 2953-2965).
+RG_HDI void record_car_hit(CarState& hitter, uint32_t hitter_id, uint32_t victim_id, bool is_demo, uint8_t hitter_team,
+                           const EventStream& events) {
     const uint32_t k = ((victim_id - hitter_id) & 7u) - 1u;
     if (is_demo) {
         hitter.bump_event_demos[k] = static_cast<uint8_t>(hitter.bump_event_demos[k] + 1u);
     } else {
         hitter.bump_event_bumps[k] = static_cast<uint8_t>(hitter.bump_event_bumps[k] + 1u);
+    }
+    if (events.windows) {
+        PhysicsEvent e = new_event(kEventCarBump);
+        e.car_id = hitter_id;
+        e.other_car_id = victim_id;
+        e.team = hitter_team;
+        e.is_demo = is_demo ? 1 : 0;
+        e.car_on_ground = hitter.is_on_ground;
+        e.position = hitter.pos;
+        e.car_velocity = hitter.vel;
+        emit_event_for_car(events, hitter_id, e);
     }
 }
 RG_HDI void ue3_rotator_axes(const Ue3Rotator& r, V3& x, V3& y, V3& z) {
@@ -1180,8 +1194,8 @@ RG_HDI bool should_demolish(const CarState& a, const CarConfig& acfg, V3 a_start
 
 // The hitter's bumper cone: a demolition when supersonic (not this tick's path: the demolition test above already
 // ran), else a bump impulse queued on the victim (reference BumpCone).
-RG_HDI bool bump_cone(CarState& h, uint32_t hid, const CarConfig& hcfg, V3 h_start_vel, CarState& v, uint32_t vid,
-                      const CarConfig& vcfg, const TickConfig& tc) {
+RG_HDI bool bump_cone(CarState& h, uint32_t hid, uint8_t hteam, const CarConfig& hcfg, V3 h_start_vel, CarState& v,
+                      uint32_t vid, const CarConfig& vcfg, const TickConfig& tc) {
     const bool bumper = in_forward_cone(h.pos, h.rot, hcfg, v.pos, v.rot, vcfg, false, 70.0f);
     if (bumper) {
         const float speed = sqrtf(len2(h_start_vel));
@@ -1214,7 +1228,7 @@ RG_HDI bool bump_cone(CarState& h, uint32_t hid, const CarConfig& hcfg, V3 h_sta
     }
     h.car_contact.other_car_id = vid;
     h.car_contact.cooldown_timer = tc.bump_cooldown_time + tc.tick_dt * 0.5f;
-    if (bumper) record_car_hit(h, hid, vid, false);
+    if (bumper) record_car_hit(h, hid, vid, false, hteam, tc.events);
     return false;
 }
 
@@ -1242,11 +1256,11 @@ RG_HDI bool car_car_directional(CarState& h, uint32_t hid, uint8_t hteam, const 
     if (demo && !tc.enable_team_demos) demo = hteam != vteam;
     if (demo) {
         demolish_car(v, tc);
-        record_car_hit(h, hid, vid, true);
+        record_car_hit(h, hid, vid, true, hteam, tc.events);
         return true;
     }
     if (in_cooldown) return false;
-    return bump_cone(h, hid, hcfg, vel, v, vid, vcfg, tc);
+    return bump_cone(h, hid, hteam, hcfg, vel, v, vid, vcfg, tc);
 }
 
 // A car pair's contact for this tick (reference ResolveCarCarCollisionImpl<shared rows>): the retained manifold, the
@@ -1290,6 +1304,19 @@ RG_NOINL void car_car_resolve(CarState& a, uint32_t id_a, uint8_t team_a, const 
         }
     }
     car_car_rows(a, b, ca, cb, tc, pa, pb, tc.tick_dt, ia, ib, m, rows);
+    if (m.count > 0) {
+        // the pair's rows write each car's velocity, angular velocity and origin back (reference
+        // EmitSharedCarCarContactRows, env_step.hpp:665-680): unchanged for finite values except the origin's uu copy,
+        // recomputed from bt, which later bumps and the car's events read
+        auto write_back = [](CarState& c) {
+            const V3 dv = c.vel - c.vel;
+            if (dv.x != 0.0f || dv.y != 0.0f || dv.z != 0.0f) car_set_vel_uu(c, c.vel + dv);
+            c.ang_vel = c.ang_vel + (c.ang_vel - c.ang_vel);
+            car_set_pos_bt(c, c.pos_bt + (c.pos_bt - c.pos_bt));
+        };
+        write_back(a);
+        write_back(b);
+    }
 }
 
 }  // namespace rg

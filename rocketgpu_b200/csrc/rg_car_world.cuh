@@ -368,6 +368,15 @@ struct CarWorldContactResult {
     bool hit;
     V3 latest_normal;
 };
+// The query's car-world events: one per manifold point made into rows, with the point's normal, and the car's
+// position, velocity and ground flag (reference ContactAccumulator::add and its event, arena_geometry.hpp:21-46,
+// arena_ball.hpp:563-573); the arena emits them where the reference's query runs.
+struct MeshContactEvents {
+    uint32_t count;
+    uint8_t on_ground;
+    V3 pos, vel;
+    V3 normal[4];
+};
 
 // The car's contacts with the arena mesh for this tick: refresh the retained manifold, collect candidates from the
 // triangles the box overlaps, merge them into the manifold and emit rows (body index `body`, source tag 100).
@@ -378,10 +387,16 @@ struct CarWorldContactResult {
 template <class Rows>
 RG_NOINL CarWorldContactResult car_mesh_contacts(const CarState& c, const CarConfig& cfg, CarWorldScratch& ws,
                                                bool listed, const MeshDevice& mesh, const TickConfig& tc, int body,
-                                               Rows& rows) {
+                                               Rows& rows, MeshContactEvents* events = nullptr) {
     CarWorldContactResult res;
     res.hit = false;
     res.latest_normal = V3{0.0f, 0.0f, 1.0f};
+    if (events) {
+        events->count = 0;
+        events->on_ground = c.is_on_ground;
+        events->pos = c.pos;
+        events->vel = c.vel;
+    }
     if (!listed) {
         ws.count = 0;
         return res;
@@ -515,6 +530,7 @@ RG_NOINL CarWorldContactResult car_mesh_contacts(const CarState& c, const CarCon
         const V3 pwa = car_world_point(f, r, u, pos, p.local_a);
         const V3 rel_bt = pwa - pos;
         res.hit = true;
+        if (events) events->normal[events->count++] = p.normal;
         const V3 ang_bt = mul_rows(i0, i1, i2, cross(rel_bt, p.normal));
         const float pen_uu = fmax_(0.0f, -p.distance) * 50.0f;
         V3 split_ang_uu{0.0f, 0.0f, 0.0f};

@@ -196,12 +196,22 @@ RG_HDI void pad_touch_step(PadState& pad, int p, CarState& c, uint32_t car_id, b
 RG_HDI void pad_give(CarState* cars, int car_base, int max_cars, PadState& pad, int p, uint32_t car_id,
                      const TickConfig& tc) {
     CarState& c = cars[static_cast<int>(car_id - 1u) - car_base];
+    const float boost_before = c.boost;
     car_set_boost_amount(c, fmin_(tc.boost_max / 100.0f, car_boost_amount(c) + (pad.is_big ? 1.0f : 0.12f)));
     pad.is_active = 0;
     pad.cooldown = (pad.is_big ? tc.boost_pad_cooldown_big : tc.boost_pad_cooldown_small) - tc.tick_dt;
     pad.pickup_frac_q = pad_frac_q(tc.frame_frac);
     for (int i = 0; i < max_cars; ++i)
         if (cars[i].boost_pad_touching == p + 1) cars[i].boost_pad_touching = 0;
+    if (tc.events.windows) {
+        PhysicsEvent e = new_event(kEventBoostPickup);
+        e.car_id = car_id;
+        e.pad_index = static_cast<uint32_t>(p);
+        e.is_big_pad = pad.is_big;
+        e.boost_before = boost_before;
+        e.boost_after = c.boost;
+        emit_event(tc.events, static_cast<uint32_t>(car_base / max_cars), e);
+    }
 }
 // More than one pad hit in one tick: visit them in order of entry (reference BoostPadSweepTouchSteps, :2587-2637).
 RG_HDI void pad_sweep_touch_steps(CarState* cars, int car_base, int max_cars, int slot, PadState* pads,

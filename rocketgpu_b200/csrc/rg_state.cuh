@@ -4,6 +4,7 @@
 #pragma once
 
 #include <stddef.h>
+#include <string.h>
 
 #include "rg_math.cuh"
 #include "rocketgpu_b200.h"
@@ -72,6 +73,40 @@ struct ArenaRules {
 
 struct KickoffSettledRow;  // rg_reset.cuh
 
+// Physics events (reference PhysicsEventType / PhysicsEvent / PhysicsEventWindow / PhysicsEventStream,
+// rocketgpu.h:44-98), byte-identical to rg_physics_event / rg_physics_event_window.
+enum : uint8_t {
+    kEventBallTouchStart = 0,
+    kEventBallWorldContact = 1,
+    kEventCarWorldContact = 2,
+    kEventBoostPickup = 3,
+    kEventCarBump = 4,
+    kEventGoal = 5,
+};
+struct PhysicsEvent {
+    uint64_t tick;
+    uint8_t type;
+    uint32_t car_id, other_car_id;
+    int32_t team;
+    uint32_t pad_index;
+    uint8_t car_on_ground, is_big_pad, is_demo;
+    V3 position, normal, car_velocity, ball_position, ball_velocity;
+    float boost_before, boost_after;
+};
+struct PhysicsEventWindow {
+    uint64_t tick;
+    uint32_t count, overflow;
+};
+static_assert(sizeof(PhysicsEvent) == sizeof(rg_physics_event) && sizeof(PhysicsEvent) == 104, "PhysicsEvent layout");
+static_assert(offsetof(PhysicsEvent, position) == 32 && offsetof(PhysicsEvent, boost_after) == 96, "PhysicsEvent");
+static_assert(sizeof(PhysicsEventWindow) == sizeof(rg_physics_event_window), "PhysicsEventWindow layout");
+// The stream a batch writes: records[env * capacity + k] and windows[env] in device memory; off when windows is null.
+struct EventStream {
+    PhysicsEvent* records;
+    PhysicsEventWindow* windows;
+    uint32_t capacity, env_count, cars_per_env, goal_only;
+};
+
 struct TickConfig {
     float tick_dt;
     float gravity_z;
@@ -108,6 +143,32 @@ struct TickConfig {
     const int32_t* settled_entry;  // per car slot: its entry, or -1
     const BallState* settled_ball;
     int32_t settled_spawns;  // rows per entry (kickoff spots): max(max_cars_per_env, 5)
+    EventStream events;      // physics events, or all zero
 };
+
+// A new event of `type` with the reference's member defaults (every field zero, team -1).
+RG_HDI PhysicsEvent new_event(uint8_t type) {
+    PhysicsEvent e;
+    memset(&e, 0, sizeof(e));
+    e.type = type;
+    e.team = -1;
+    return e;
+}
+// reference PhysicsEventStream::Emit / EmitForCar (rocketgpu.h:83-97): the env's window stamps the tick; a full
+// window sets its overflow flag instead.
+RG_HDI void emit_event(const EventStream& s, uint32_t env, PhysicsEvent e) {
+    if (s.goal_only && e.type != kEventGoal) return;
+    if (!s.windows || env >= s.env_count) return;
+    PhysicsEventWindow& w = s.windows[env];
+    e.tick = w.tick;
+    if (w.count >= s.capacity) {
+        w.overflow = 1;
+        return;
+    }
+    s.records[static_cast<size_t>(env) * s.capacity + w.count++] = e;
+}
+RG_HDI void emit_event_for_car(const EventStream& s, uint32_t id, const PhysicsEvent& e) {
+    if (id && s.cars_per_env) emit_event(s, (id - 1) / s.cars_per_env, e);
+}
 
 }  // namespace rg

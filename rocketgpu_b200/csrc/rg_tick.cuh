@@ -137,7 +137,9 @@ RG_HDI void ball_finish(BallState& b) {
 
 // Goal test against the mouth planes and the render-frame bookkeeping (reference StepEnvTail, env_step.hpp:7006-7045;
 // CountdownUpdateTimers :6516-6537). The countdown's end re-enables driving of the arena's first `count` car slots.
-RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState* cars = nullptr, int count = 0) {
+// event_env >= 0: a goal is a goal event of that arena.
+RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState* cars = nullptr, int count = 0,
+                     int event_env = -1) {
     ball_finish(b);
     if (c.enable_scoring && c.rules) {
         // a custom arena's goals (reference ScoreArenaRulesGoals, env_step.hpp:6951-6966)
@@ -172,6 +174,14 @@ RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState*
         }
         env.goal_latched = env.goal_scored_this_tick;
     }
+    if (env.goal_scored_this_tick && c.events.windows && event_env >= 0) {
+        // reference StepEnvTail, env_step.hpp:7026-7033
+        PhysicsEvent e = new_event(kEventGoal);
+        e.team = env.last_scored_team;
+        e.ball_position = b.pos;
+        e.ball_velocity = b.vel;
+        emit_event(c.events, static_cast<uint32_t>(event_env), e);
+    }
     env.frame_ticks += 1;
     const float frame_frac = c.frame_frac;
     if (frame_frac >= 0.0f) {
@@ -201,7 +211,8 @@ RG_HDI void env_tail(EnvState& env, BallState& b, const TickConfig& c, CarState*
 
 // World step, ball-only arena (reference WorldStepSoccar with count == 0, env_step.hpp:4727-5623): activation,
 // arena contacts, gravity, integration and Bullet's deactivation timer.
-RG_HDI void ball_world_step(BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& mesh) {
+RG_HDI void ball_world_step(BallState& b, BallWorldScratch& s, const TickConfig& c, const MeshDevice& mesh,
+                            int event_env = -1) {
     const float sub_dt = c.tick_dt;  // one world substep per tick
     const bool vehicle_woke = (b.sleeping & 4u) != 0;
     b.sleeping &= 3u;
@@ -241,7 +252,7 @@ RG_HDI void ball_world_step(BallState& b, BallWorldScratch& s, const TickConfig&
     // arena contacts: a sleeping ball keeps its manifold untouched
     BallContactRows rows;
     rows.split_count = rows.vel_count = rows.fric_count = 0;
-    if (awake) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
+    if (awake) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows, event_env);
     if (pred_hit) ball_predictive_rows(b, c, pred_n, pred_dist, ext_delta, solver_vel_bt, sub_dt, rows);
     if (rows.vel_count || rows.fric_count) {
         V3 dl, da;
@@ -264,13 +275,15 @@ RG_HDI void ball_world_step(BallState& b, BallWorldScratch& s, const TickConfig&
 }
 
 // One tick of one ball-only arena (reference StepEnvGeneric, env_step.hpp:7088-7180).
+// env_idx: the arena's index for physics events.
 RG_HDI void arena_tick(EnvState& env, BallState& b, BallWorldScratch& s, const TickConfig& c,
-                       const MeshDevice& mesh) {
+                       const MeshDevice& mesh, int env_idx = -1) {
+    if (c.events.windows && env_idx >= 0) c.events.windows[env_idx].tick = env.tick;
     env.goal_scored_this_tick = 0;
     ball_tick_start_quantize(b, c);
     ball_clamp_and_drag(b, c);
-    ball_world_step(b, s, c, mesh);
-    env_tail(env, b, c);
+    ball_world_step(b, s, c, mesh, env_idx);
+    env_tail(env, b, c, nullptr, 0, env_idx);
 }
 
 // ---- arenas with cars --------------------------------------------------------------------------------------------
@@ -1245,6 +1258,7 @@ struct CarStage {
     uint8_t wheel_meets_car[4];  // the wheel's ray meets another car's box (0 for a demolished car)
     BallCarScratch ball_manifold;  // the car/ball manifold after this tick's geometry (car_ball_stage)
     uint32_t ball_staged;          // ball_manifold holds this tick's update
+    MeshContactEvents mesh_events;  // the query's car-world events (when events are on)
 };
 
 // A car's broadphase proxy: its box now and at the pose this tick's tick-start velocities predict (reference
@@ -1294,9 +1308,11 @@ RG_HDI void car_stage_compute(CarState& car, const CarConfig& cfg, WheelRuntime&
     st.rows.nv = st.rows.nf = st.rows.ns = 0;
     st.res.hit = false;
     st.res.latest_normal = V3{0.0f, 0.0f, 1.0f};
+    st.mesh_events.count = 0;
     if (st.mesh_ran) {
         st.ws = ws_in;
-        st.res = car_mesh_contacts(car, cfg, st.ws, true, mesh, c, slot, st.rows);
+        st.res = car_mesh_contacts(car, cfg, st.ws, true, mesh, c, slot, st.rows,
+                                   c.events.windows ? &st.mesh_events : nullptr);
     }
 }
 
@@ -1447,14 +1463,15 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
         if (!pre[i].is_demoed && !car.just_respawned)
             commit_ball_hit_from_manifold(b, car, bcs[i], static_cast<uint32_t>(A.car_base + i + 1), env_tick,
                                           hit_car_pos[i], hit_car_rot[i], hit_ball_pos, snap.car_start_vel[i],
-                                          snap.ball_start_vel);
+                                          snap.ball_start_vel, A.teams[i], c.events);
     }
     // the ball's arena contacts (reference env_step.hpp:5219-5290): a sleeping ball a car touched is awake now,
     // and looks at the arena when it still holds arena contact points
     const bool awake_after = awake || bc.nv > 0 || bc.nf > 0 || bc.ns > 0;
     BallContactRows rows;
     rows.split_count = rows.vel_count = rows.fric_count = 0;
-    if (awake_after && (awake || s.count != 0)) ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows);
+    if (awake_after && (awake || s.count != 0))
+        ball_mesh_contacts(b, s, c, mesh, ext_delta, solver_vel_bt, sub_dt, rows, A.car_base / A.max_cars);
     // the cars' arena contacts, in slot order
     CarWorldRows cr;
     cr.nv = cr.nf = cr.ns = 0;
@@ -1471,8 +1488,11 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
         }
         if (!listed && cws[i].count == 0) continue;
         CarWorldContactResult res;
+        MeshContactEvents ev;
+        const MeshContactEvents* events = nullptr;
         if (!stages) {
-            res = car_mesh_contacts(car, A.cfgs[i], cws[i], listed, mesh, c, i, cr);
+            res = car_mesh_contacts(car, A.cfgs[i], cws[i], listed, mesh, c, i, cr, c.events.windows ? &ev : nullptr);
+            events = &ev;
         } else if (!listed) {
             cws[i].count = 0;  // what the query does for an unlisted manifold
             continue;
@@ -1480,6 +1500,18 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
             cws[i] = stages[i].ws;
             append_car_rows(cr, stages[i].rows);
             res = stages[i].res;
+            events = &stages[i].mesh_events;
+        }
+        if (c.events.windows) {
+            for (uint32_t k = 0; k < events->count; ++k) {
+                PhysicsEvent e = new_event(kEventCarWorldContact);
+                e.car_id = static_cast<uint32_t>(A.car_base + i + 1);
+                e.position = events->pos;
+                e.car_velocity = events->vel;
+                e.car_on_ground = events->on_ground;
+                e.normal = events->normal[k];
+                emit_event_for_car(c.events, e.car_id, e);
+            }
         }
         if (res.hit) {
             car_record_world_surface(car, true);
@@ -1624,6 +1656,7 @@ RG_HDI void arena_tick_begin(EnvState& env, BallState& b, const ArenaCars& A, co
     const int count = A.count;
     update_game_visit_order(env, A.cars, count);
     pick_respawn_spots(A, b, env, c, respawn_seed, env_idx);
+    if (c.events.windows) c.events.windows[env_idx].tick = env.tick;  // reference StepEnvPreTickEnvState, :6694-6696
     env.goal_scored_this_tick = 0;
     ball_tick_start_quantize(b, c);
     as.ball_start_vel = b.vel;
@@ -1639,6 +1672,7 @@ RG_HDI void car_tick_pre(CarState& car, const CarControls& k, const CarConfig& c
     r.vel_bt = car.vel_bt;
     r.ang_vel = car.ang_vel;
     r.pushes.count = 0;
+    r.pushes.world_event = 0u;
 }
 
 // The cars of an arena whose vehicle update is independent of the other cars': no other car can be under one of its
@@ -1704,6 +1738,21 @@ RG_HDI void arena_tick_finish(EnvState& env, BallState& b, BallWorldScratch& s, 
         if ((left >> i) & 1u)
             car_stage_compute(A.cars[i], A.cfgs[i], A.wheels[i], cws[i], c, mesh, i, recs[i].vel_bt, recs[i].ang_vel,
                               stages[i]);
+    if (c.events.windows) {
+        // the vehicle updates' car-world events, in the game's car order (each update emits its own in the reference)
+        for (int k = 0; k < count; ++k) {
+            const int i = order[k];
+            const WheelBallPushes& p = recs[i].pushes;
+            if (!p.world_event) continue;
+            PhysicsEvent e = new_event(kEventCarWorldContact);
+            e.car_id = static_cast<uint32_t>(A.car_base + i + 1);
+            e.position = p.world_event_pos;
+            e.car_velocity = p.world_event_vel;
+            e.car_on_ground = p.world_event_on_ground;
+            e.normal = p.world_event_normal;
+            emit_event(c.events, static_cast<uint32_t>(A.car_base / A.max_cars), e);
+        }
+    }
     for (int k = 0; k < count; ++k) apply_wheel_ball_pushes(b, recs[order[k]].pushes, c);
     PreContactCar pre[8];
     world_step_cars(b, s, bp, cws, bcs, c, mesh, A, pre, snap, env.tick, stages);
@@ -1745,7 +1794,7 @@ RG_HDI void arena_tick_tail(EnvState& env, BallState& b, const ArenaCars& A, con
         if (!car.is_demoed && car.driving_disabled) --car.driving_disabled;
     }
     apply_ball_extra_hits(b, A.cars, count, c);
-    env_tail(env, b, c, A.cars, count);
+    env_tail(env, b, c, A.cars, count, A.car_base / A.max_cars);
 }
 
 // ---- env commands ------------------------------------------------------------------------------------------------

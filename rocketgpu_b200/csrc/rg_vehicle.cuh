@@ -1044,6 +1044,11 @@ RG_HDI void car_impulse_at_point_bt(CarState& c, const CarConfig& cfg, float mas
 struct WheelBallPushes {
     int32_t count;
     V3 point_bt[4], normal[4];
+    // the update's car-world event (a wheel newly on the arena, when events are on), which the arena emits in the
+    // game's car order: its normal, and the car's position, velocity and ground flag after the update
+    uint32_t world_event;
+    uint8_t world_event_on_ground;
+    V3 world_event_normal, world_event_pos, world_event_vel;
 };
 RG_HDI void apply_wheel_ball_pushes(BallState& ball, const WheelBallPushes& p, const TickConfig& tc) {
     for (int k = 0; k < p.count; ++k) {
@@ -1061,6 +1066,7 @@ RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cf
                            WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, const WheelOthers& oth,
                            WheelBallPushes& pushes, const RayHit* mesh_hits = nullptr) {
     pushes.count = 0;
+    pushes.world_event = 0u;
     const float dt = tc.tick_dt;
     c.demo_no_contact_response = c.is_demoed ? 1 : 0;
     if (c.is_demoed) return;
@@ -1314,6 +1320,33 @@ RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cf
     wr.accumulated_ang_accel = f.queued_ang_accel;
     wr.accumulated_torque_bt = f.queued_torque_bt;
     wr.solver_time_step = dt;
+    if (tc.events.windows) {
+        // the wheel on the arena with the most upward normal, unless a wheel stood on the same triangle with the same
+        // normal last tick (reference PreTickCar, env_step.hpp:3426-3469)
+        bool has = false;
+        V3 normal{0.0f, 0.0f, 0.0f};
+        int32_t id = -1;
+        for (int i = 0; i < 4; ++i) {
+            if (wh[i].is_in_contact && wh[i].is_in_contact_with_world && (!has || wh[i].contact_normal_ws.z > normal.z)) {
+                has = true;
+                normal = wh[i].contact_normal_ws;
+                id = wh[i].ground_static_id;
+            }
+        }
+        bool previous = false;
+        if (has && c.tick_count_since_update != 0) {
+            for (int i = 0; i < 4; ++i) {
+                const V3 old = wr.event_world_normals[i];
+                previous = previous || (wr.event_world_ids[i] == id && old.x == normal.x && old.y == normal.y &&
+                                        old.z == normal.z);
+            }
+        }
+        pushes.world_event = has && !previous ? 1u : 0u;
+        pushes.world_event_normal = normal;
+        pushes.world_event_pos = c.pos;
+        pushes.world_event_vel = c.vel;
+        pushes.world_event_on_ground = c.is_on_ground;
+    }
     for (int i = 0; i < 4; ++i) {
         const bool world = wh[i].is_in_contact && wh[i].is_in_contact_with_world;
         wr.event_world_ids[i] = world ? wh[i].ground_static_id : -1;

@@ -47,6 +47,8 @@ def lib():
         L.orc_step_with_controls.argtypes = [vp, vp, i32, i32]
         L.orc_step_with_commands.argtypes = [vp, vp, i32, vp, i32, i32]
         L.orc_car_preset.argtypes = [ctypes.c_int, vp]
+        L.orc_set_physics_event_stream.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_int]
+        L.orc_physics_event_sizes.argtypes = [vp]
         L.orc_default_states.argtypes = [vp, vp, vp, vp, vp]
         _lib = L
     return _lib
@@ -126,6 +128,19 @@ class OracleSim:
 
     def reset_to_kickoff(self, seed: int = 0):
         _check(lib().orc_reset_to_kickoff(self.h, seed))
+
+    def set_physics_event_stream(self, capacity: int, goal_only: bool = False):
+        """The reference's event stream on host arrays the oracle writes: returns (records, windows), uint8 arrays of
+        env_count * capacity * 104 and env_count * 16 bytes (capacity 0: off, returns None)."""
+        if capacity == 0:
+            _check(lib().orc_set_physics_event_stream(self.h, None, None, 0, 0))
+            self._events = None
+            return None
+        n = self.env_count
+        self._events = (np.zeros(n * capacity * 104, np.uint8), np.zeros(n * 16, np.uint8))
+        _check(lib().orc_set_physics_event_stream(self.h, _ptr(self._events[0]), _ptr(self._events[1]), capacity,
+                                                  1 if goal_only else 0))
+        return self._events
 
     def apply_env_commands(self, cmds: np.ndarray):
         c = np.ascontiguousarray(cmds, np.uint8).reshape(-1, CMD_BYTES)
