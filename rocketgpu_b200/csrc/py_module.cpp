@@ -148,6 +148,13 @@ class BatchSim {
     }
     void reset_to_kickoff(uint64_t seed, uintptr_t s) { check(rg_batch_reset_to_kickoff(b_, seed, stream_of(s))); }
     void synchronize(uintptr_t s) { check(rg_batch_synchronize(b_, stream_of(s))); }
+    // reference binding set_physics_event_stream (python/rocketgpu_bindings.cpp:832-845): device addresses; zeros
+    // turn the stream off
+    void set_physics_event_stream(uintptr_t records, uintptr_t windows, uint32_t capacity, bool goal_only) {
+        check(rg_batch_set_physics_event_stream(b_, reinterpret_cast<rg_physics_event*>(records),
+                                                reinterpret_cast<rg_physics_event_window*>(windows), capacity,
+                                                goal_only ? 1 : 0));
+    }
     py::dict device_view() {
         rg_device_view v{};
         check(rg_batch_device_view(b_, &v));
@@ -335,5 +342,20 @@ PYBIND11_MODULE(rocketgpu_py_b200, m) {
              py::arg("control_stride"), py::arg("device_env_commands_by_tick"), py::arg("env_command_stride"),
              py::arg("ticks"), py::arg("stream") = 0)
         .def("reset_to_kickoff", &BatchSim::reset_to_kickoff, py::arg("seed") = 0, py::arg("stream") = 0)
-        .def("synchronize", &BatchSim::synchronize, py::arg("stream") = 0);
+        .def("synchronize", &BatchSim::synchronize, py::arg("stream") = 0)
+        .def("set_physics_event_stream", &BatchSim::set_physics_event_stream, py::arg("records"), py::arg("windows"),
+             py::arg("capacity"), py::arg("goal_only") = false,
+             "Pass zeros to disable; synchronise before freeing the buffers.");
+    // reference physics_event_layout (python/rocketgpu_bindings.cpp:77-86)
+    m.def("physics_event_layout", [] {
+        py::dict d;
+        d["record_size"] = sizeof(rg_physics_event);
+        d["window_size"] = sizeof(rg_physics_event_window);
+        d["type_offset"] = offsetof(rg_physics_event, type);
+        d["velocity_offset"] = offsetof(rg_physics_event, ball_velocity);
+        d["count_offset"] = offsetof(rg_physics_event_window, count);
+        d["overflow_offset"] = offsetof(rg_physics_event_window, overflow);
+        d["goal_type"] = 5;
+        return d;
+    });
 }

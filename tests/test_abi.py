@@ -136,8 +136,11 @@ def test_pybind_module_mirrors_the_reference_binding(arena_mesh):
                  "download_env_states", "download_boost_pad_states", "upload_state_array", "download_state_array",
                  "apply_env_commands", "apply_env_commands_device", "step", "step_with_device_controls",
                  "step_with_device_commands", "reset_to_kickoff", "synchronize", "internal_state_layout",
-                 "download_internal_state", "upload_internal_state"):
+                 "download_internal_state", "upload_internal_state", "set_physics_event_stream"):
         assert hasattr(m.BatchSim, name), name
+    assert m.physics_event_layout() == {"record_size": 104, "window_size": 16, "type_offset": 8,
+                                        "velocity_offset": 80, "count_offset": 8, "overflow_offset": 12,
+                                        "goal_type": 5}
     layout = m.ArenaLayout()
     for name in ("meshes", "boost_pads", "goals", "kickoff_spawns", "respawn_spawns", "ball_spawn"):
         assert hasattr(layout, name), name
