@@ -1061,6 +1061,36 @@ RG_HDI void apply_wheel_ball_pushes(BallState& ball, const WheelBallPushes& p, c
     }
 }
 
+// The update's car-world event: the wheel on the arena with the most upward normal, unless a wheel stood on the same
+// triangle with the same normal last tick (reference PreTickCar, env_step.hpp:3426-3469). Kept out of line: only a
+// batch with an event stream calls it.
+RG_NOINL void wheel_world_event(const CarState& c, const WheelRuntime& wr, const WheelStep* wh,
+                                WheelBallPushes& pushes) {
+    bool has = false;
+    V3 normal{0.0f, 0.0f, 0.0f};
+    int32_t id = -1;
+    for (int i = 0; i < 4; ++i) {
+        if (wh[i].is_in_contact && wh[i].is_in_contact_with_world && (!has || wh[i].contact_normal_ws.z > normal.z)) {
+            has = true;
+            normal = wh[i].contact_normal_ws;
+            id = wh[i].ground_static_id;
+        }
+    }
+    bool previous = false;
+    if (has && c.tick_count_since_update != 0) {
+        for (int i = 0; i < 4; ++i) {
+            const V3 old = wr.event_world_normals[i];
+            previous = previous || (wr.event_world_ids[i] == id && old.x == normal.x && old.y == normal.y &&
+                                    old.z == normal.z);
+        }
+    }
+    pushes.world_event = has && !previous ? 1u : 0u;
+    pushes.world_event_normal = normal;
+    pushes.world_event_pos = c.pos;
+    pushes.world_event_vel = c.vel;
+    pushes.world_event_on_ground = c.is_on_ground;
+}
+
 // `mesh_hits`: the four wheels' arena-mesh rays cast ahead (wheel_mesh_ray_ahead), or null to cast them here.
 RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cfg, const TickConfig& tc,
                            WheelRuntime& wr, const BallState& ball, const MeshDevice& mesh, const WheelOthers& oth,
@@ -1320,33 +1350,7 @@ RG_NOINL void vehicle_update(CarState& c, CarControls k_raw, const CarConfig& cf
     wr.accumulated_ang_accel = f.queued_ang_accel;
     wr.accumulated_torque_bt = f.queued_torque_bt;
     wr.solver_time_step = dt;
-    if (tc.events.windows) {
-        // the wheel on the arena with the most upward normal, unless a wheel stood on the same triangle with the same
-        // normal last tick (reference PreTickCar, env_step.hpp:3426-3469)
-        bool has = false;
-        V3 normal{0.0f, 0.0f, 0.0f};
-        int32_t id = -1;
-        for (int i = 0; i < 4; ++i) {
-            if (wh[i].is_in_contact && wh[i].is_in_contact_with_world && (!has || wh[i].contact_normal_ws.z > normal.z)) {
-                has = true;
-                normal = wh[i].contact_normal_ws;
-                id = wh[i].ground_static_id;
-            }
-        }
-        bool previous = false;
-        if (has && c.tick_count_since_update != 0) {
-            for (int i = 0; i < 4; ++i) {
-                const V3 old = wr.event_world_normals[i];
-                previous = previous || (wr.event_world_ids[i] == id && old.x == normal.x && old.y == normal.y &&
-                                        old.z == normal.z);
-            }
-        }
-        pushes.world_event = has && !previous ? 1u : 0u;
-        pushes.world_event_normal = normal;
-        pushes.world_event_pos = c.pos;
-        pushes.world_event_vel = c.vel;
-        pushes.world_event_on_ground = c.is_on_ground;
-    }
+    if (tc.events.windows) wheel_world_event(c, wr, wh, pushes);
     for (int i = 0; i < 4; ++i) {
         const bool world = wh[i].is_in_contact && wh[i].is_in_contact_with_world;
         wr.event_world_ids[i] = world ? wh[i].ground_static_id : -1;
