@@ -368,13 +368,11 @@ struct CarWorldContactResult {
     bool hit;
     V3 latest_normal;
 };
-// The query's car-world events: one per manifold point made into rows, with the point's normal, and the car's
-// position, velocity and ground flag (reference ContactAccumulator::add and its event, arena_geometry.hpp:21-46,
-// arena_ball.hpp:563-573); the arena emits them where the reference's query runs.
+// The query's car-world events: one per manifold point made into rows, with the point's normal (reference
+// ContactAccumulator::add and its event, arena_geometry.hpp:21-46, arena_ball.hpp:563-573); the arena emits them where
+// the reference's query runs, with the car's position, velocity and ground flag at that moment.
 struct MeshContactEvents {
     uint32_t count;
-    uint8_t on_ground;
-    V3 pos, vel;
     V3 normal[4];
 };
 
@@ -391,12 +389,7 @@ RG_NOINL CarWorldContactResult car_mesh_contacts(const CarState& c, const CarCon
     CarWorldContactResult res;
     res.hit = false;
     res.latest_normal = V3{0.0f, 0.0f, 1.0f};
-    if (events) {
-        events->count = 0;
-        events->on_ground = c.is_on_ground;
-        events->pos = c.pos;
-        events->vel = c.vel;
-    }
+    if (events) events->count = 0;
     if (!listed) {
         ws.count = 0;
         return res;

@@ -1506,9 +1506,9 @@ RG_NOINL void world_step_cars(BallState& b, BallWorldScratch& s, Broadphase& bp,
             for (uint32_t k = 0; k < events->count; ++k) {
                 PhysicsEvent e = new_event(kEventCarWorldContact);
                 e.car_id = static_cast<uint32_t>(A.car_base + i + 1);
-                e.position = events->pos;
-                e.car_velocity = events->vel;
-                e.car_on_ground = events->on_ground;
+                e.position = car.pos;  // as the car stands here: a pair's rows may have rewritten its uu origin
+                e.car_velocity = car.vel;
+                e.car_on_ground = car.is_on_ground;
                 e.normal = events->normal[k];
                 emit_event_for_car(c.events, e.car_id, e);
             }

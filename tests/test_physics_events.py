@@ -36,9 +36,6 @@ def _field_bits(rec):
     return out
 
 
-inexact = [0, 0]  # car-world contact positions one ulp apart, car-world contacts compared
-
-
 def _compare_events(orc_events, gpu_records, gpu_windows, n, cap):
     ev, win = _dtypes()
     ow = orc_events[1].view(win)
@@ -54,14 +51,6 @@ def _compare_events(orc_events, gpu_records, gpu_windows, n, cap):
         if k == 0:
             continue
         a, b = _field_bits(orec[e, :k]), _field_bits(grec[e, :k])
-        # a car-world contact's position is the car's uu origin at the event; the reference sometimes holds it as
-        # bt * 50 and sometimes as the tick start's quantised value there (the two differ by at most one ulp, and
-        # the step overwrites both): that field alone may differ by one ulp
-        cw = orec[e, :k]["type"] == 2
-        near = (np.abs(a["position"].astype(np.int64) - b["position"].astype(np.int64)) <= 1).all(axis=1) & cw
-        inexact[0] += int((near & (a["position"] != b["position"]).any(axis=1)).sum())
-        inexact[1] += int(cw.sum())
-        b["position"] = np.where(near[:, None], a["position"], b["position"])
         for name in a:
             diff = np.nonzero(np.any((a[name] != b[name]).reshape(k, -1), axis=1))[0]
             assert len(diff) == 0, (f"arena {e} event {diff[0]} of {k} field {name}: oracle {orec[e, diff[0]]} "
@@ -127,8 +116,7 @@ def _run(arena_mesh, n, ticks_per_launch, launches, cap, seed, goal_only=False, 
 @pytest.mark.gpu
 def test_events_match_the_reference_through_play(oracle_available, arena_mesh):
     types, overflows = _run(arena_mesh, n=64, ticks_per_launch=4, launches=90, cap=512, seed=41)
-    print("events by type", dict(zip(("touch", "ball-world", "car-world", "pickup", "bump", "goal"), types.tolist())),
-          f"car-world positions one ulp apart: {inexact[0]} of {inexact[1]}")
+    print("events by type", dict(zip(("touch", "ball-world", "car-world", "pickup", "bump", "goal"), types.tolist())))
     assert overflows == 0
     assert types[0] > 0 and types[1] > 0 and types[2] > 0 and types[3] > 0 and types[4] > 0, types
 
