@@ -54,6 +54,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 ENVS = 16384
+EVENTS = 0  # --events: physics event records per arena (0: the stream is off)
 TICKS_PER_STEP = 8
 KERNELS_PER_TICK = 7  # arena begin, car tick start, wheel rays, vehicle updates, arena finish, car post-tick, arena tail
 SETTLE_STEPS = 40
@@ -270,6 +271,7 @@ def cpu_leg(workload: str, warmup: int, steps: int, parity: bool):
         sim.set_teams(w.teams)
         sim.set_car_configs(w.car_configs(_presets()))
         sim.reset_to_kickoff(w.reset_seed)
+        events = sim.set_physics_event_stream(EVENTS) if EVENTS else None
         clock = scenarios.EpisodeClock(sim.envs(), sim.cars(), MAX_CARS, NO_TOUCH_TICKS, w.stagger_seed)
         cmds = np.zeros((TICKS_PER_STEP * ENVS, CMD_BYTES), np.uint8)
         gen = w.controls()
@@ -277,6 +279,8 @@ def cpu_leg(workload: str, warmup: int, steps: int, parity: bool):
         for k in range(total):
             block = next(gen)
             t0 = time.perf_counter()
+            if events is not None:
+                events[1].view(np.uint32).reshape(-1, 4)[:, 2:] = 0  # each window's count and overflow
             sim.step_with_commands(block, ENVS * MAX_CARS, cmds, ENVS, TICKS_PER_STEP)
             dt = time.perf_counter() - t0
             cars, envs = sim.cars(), sim.envs()
@@ -339,6 +343,10 @@ def run_ours(args, world, rank, local):
             sim.set_teams(w.teams)
             sim.set_car_configs(w.car_configs(presets))
             sim.reset_to_kickoff(w.reset_seed)
+            if EVENTS:
+                sim.events = (torch.zeros(ENVS * EVENTS * 104, dtype=torch.uint8, device="cuda"),
+                              torch.zeros(ENVS * 16, dtype=torch.uint8, device="cuda"))
+                sim.set_physics_event_stream(sim.events[0].data_ptr(), sim.events[1].data_ptr(), EVENTS)
             cmds = torch.zeros((TICKS_PER_STEP, ENVS, CMD_BYTES), dtype=torch.uint8, device="cuda")
             check(lib.rg_batch_episode_commands(sim._h, NO_TOUCH_TICKS, w.stagger_seed, 1,
                                                 ctypes.c_void_p(cmds.data_ptr()), s_handle))
@@ -355,6 +363,8 @@ def run_ours(args, world, rank, local):
 
     def step(sim, cmds, ctrl_ptr):
         if mixed:
+            if EVENTS:
+                sim.events[1].zero_()  # the windows, on the step's stream
             check(lib.rg_batch_step_with_device_commands(sim._h, ctypes.c_void_p(ctrl_ptr), cap,
                                                          ctypes.c_void_p(cmds.data_ptr()), ENVS, TICKS_PER_STEP,
                                                          s_handle))
@@ -461,7 +471,7 @@ def run_ours(args, world, rank, local):
         else "synthetic (seeded ball states)",
         "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
                    "settle_steps": settle, "l2": "256 MiB flush before every timed step",
-                   "parallelism": f"arena shards x{world}"},
+                   "parallelism": f"arena shards x{world}", **({"events_per_arena": EVENTS} if EVENTS else {})},
         "latency_ms_per_step": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                                 "max": float(np.max(step_ms)), "e2e_p50": float(np.percentile(e2e_ms, 50)),
                                 "e2e_p99": float(np.percentile(e2e_ms, 99))},
@@ -725,10 +735,13 @@ def main():
                     help="reference arm: its CPU BatchSim (default) or its own CUDA build (the plain GPU bar)")
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--events", type=int, default=0,
+                    help="physics event stream on, this many records per arena (mixed workload; 0: off)")
     ap.add_argument("--arenas", type=int, default=ENVS, help="arenas per GPU (smaller cases for profiling)")
     ap.add_argument("--rate", type=float, default=1000.0, help="serving: offered step requests per second")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving: seconds per policy")
     args = ap.parse_args()
+    globals()["EVENTS"] = args.events
     if args.arenas != ENVS:
         globals()["ENVS"] = args.arenas
         for k in WORKLOADS:
