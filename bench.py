@@ -656,7 +656,8 @@ def run_reference(args, world, rank):
         "data": "synthetic (seeded arenas, bodies, controls and episode resets)" if args.workload == "mixed"
         else "synthetic (seeded ball states)",
         "config": {"workload": WORKLOADS[args.workload], "arenas_per_gpu": ENVS, "ticks_per_step": TICKS_PER_STEP,
-                   "settle_steps": SETTLE_STEPS if args.workload == "mixed" else 0},
+                   "settle_steps": SETTLE_STEPS if args.workload == "mixed" else 0,
+                   **({"events_per_arena": EVENTS} if EVENTS else {})},
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
